@@ -1,0 +1,217 @@
+/*
+ * gell.h — C ABI of gell_b200, a B200 (sm_100a) implementation of the Gell per-timestep hot path:
+ * Morton-sorted cell-list mechanics (FM), LOD x/y/z Thomas reaction-diffusion with cell uptake
+ * (LOD) and stochastic Ki-67 birth/death with stream compaction (PD).
+ *
+ * The reference (PhantomOtter/Gell) is a header-only CUDA C++ program with no FFI.  Its entry
+ * points are C++ member functions and free functions that take thrust::device_vector<Cell>&;
+ * each function below names the reference interface it replaces (file:line in the reference
+ * project).  Everything here is plain C: opaque context, plain pointers and sizes, status codes.
+ *
+ * Conventions
+ *   - Every call returns gell_status (0 = ok, negative = error).  The message of the last error
+ *     of a context is available from gell_last_error().
+ *   - Calls are ordered on the context's CUDA stream (gell_set_stream).  Calls that return a
+ *     host-visible value (a cell count, an exported buffer on the host) synchronise that stream;
+ *     the others do not.
+ *   - A context is not thread-safe: one host thread drives it at a time.
+ *   - Device pointers passed in must be on the context's device.
+ */
+#ifndef GELL_B200_GELL_H
+#define GELL_B200_GELL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GELL_ABI_VERSION 1
+
+typedef enum gell_status {
+    GELL_OK = 0,
+    GELL_ERR_INVALID_ARG = -1,   /* bad pointer, size or parameter */
+    GELL_ERR_CAPACITY = -2,      /* more cells than max_cell_num */
+    GELL_ERR_CUDA = -3,          /* a CUDA runtime call failed; see gell_last_error */
+    GELL_ERR_NO_DEVICE = -4,     /* no CUDA device visible */
+    GELL_ERR_TIMEOUT = -5,       /* a bounded device-side wait gave up */
+    GELL_ERR_STATE = -6,         /* call not valid in the current context state */
+    GELL_ERR_UNSUPPORTED = -7,   /* parameter outside what this build supports */
+    GELL_ERR_ALLOC = -8          /* device or host allocation failed */
+} gell_status;
+
+/*
+ * One cell, byte-for-byte the reference's `struct Cell` (include/Cells.cuh:9-47), 72 bytes:
+ * sign@0 (bool), mesh_idx@4, pos@8, force@20, oldforce@32, r@44, V@48, Vf@52, Vcs@56, Vns@60,
+ * phase@64, cell_clock@68.  Import/export use this layout so a reference host loop can hand its
+ * thrust::device_vector<Cell> storage (or a host copy) straight to gell_cells_import/export.
+ */
+typedef struct gell_cell {
+    uint8_t sign;          /* alive flag (reference: bool sign) */
+    uint8_t _pad[3];
+    int32_t mesh_idx;      /* x + y*N + z*N*N of the cell's voxel */
+    float pos[3];          /* um */
+    float force[3];
+    float oldforce[3];
+    float r;               /* radius, um */
+    float V, Vf, Vcs, Vns; /* total, fluid, cytoplasmic, nuclear volume, um^3 */
+    int32_t phase;         /* 0 quiescent,1 premitotic,2 postmitotic,3 apoptotic,4/5 necrotic,-1 unused */
+    float cell_clock;      /* min */
+} gell_cell;
+
+/* RNG used by the birth step. */
+typedef enum gell_rng_mode {
+    GELL_RNG_XORWOW = 0,   /* curand XORWOW, one state per array slot, curand_init(seed, slot, 0):
+                              the reference's draws (include/RandomFunctions.cuh:13-31) */
+    GELL_RNG_PHILOX = 1    /* stateless Philox4x32-10 keyed by (seed), counter (slot, step, draw) */
+} gell_rng_mode;
+
+/* Mechanics neighbour search mode. */
+typedef enum gell_mech_mode {
+    GELL_MECH_REFERENCE = 0,  /* 27 bins of size voxel_length and the reference's order-dependent
+                                 cutoff (include/FMkernel.cuh:56-118), reproduced exactly */
+} gell_mech_mode;
+
+/*
+ * Runtime parameter set.  The reference has these as compile-time #defines
+ * (include/Definitions.h:7-47 and the literals inside include/Cells.cuh); gell_params_default()
+ * fills in exactly those values.  Types follow the reference: the rates that are double-typed
+ * macros there are double here, because the reference evaluates their products in double.
+ */
+typedef struct gell_params {
+    int32_t voxel_num;            /* Voxel_num: grid edge N, same on all axes (4..1023) */
+    float voxel_length;           /* Voxel_length: voxel and mechanics bin edge, um */
+    int32_t max_cell_num;         /* Max_Cell_num: cell capacity */
+    float mechanics_dt;           /* Mechanics_dt, min */
+    float diffusion_dt;           /* Diffusion_dt, min */
+    float biology_dt;             /* Biology_dt, min */
+    /* force law (include/FMkernel.cuh:56-118) */
+    float ccca;                   /* Ccca: adhesion coefficient */
+    float cccr;                   /* Cccr: repulsion coefficient */
+    double ra_ratio;              /* Ra_ratio: interaction cutoff / (r_i + r_j) */
+    float cc_max_dist;            /* Tumor_CC_Max_Dist: initial cutoff of each cell's scan */
+    /* cell model (include/Cells.cuh:74-223) */
+    float dead_uptake_factor;     /* Dead_O2_consumption_factor */
+    float default_v;              /* Default_V */
+    float o2_prolif_thres;        /* Tumor_O2_Proliferation_Thres */
+    float o2_prolif_sat;          /* Tumor_O2_Proliferation_Sat */
+    float o2_necrosis_thres;      /* Tumor_Necrosis_02_Thres */
+    float o2_necrosis_max;        /* Tumor_Necrosis_02_Max */
+    double necrosis_rate;         /* Tumor_Necrosis_Rate, 1/min */
+    double apoptosis_rate;        /* Tumor_Apoptosis_rate, 1/min */
+    double proliferation_rate;    /* Tumor_Proliferation_Rate, 1/min */
+    float duration_pre2post;      /* duration_pre2post, min */
+    float duration_post2q;        /* duration_post2q, min */
+    /* which substrate drives the Ki-67 model (the reference's oxygen mesh) */
+    int32_t o2_substrate;
+    int32_t rng_mode;             /* gell_rng_mode */
+    int32_t mech_mode;            /* gell_mech_mode */
+    int32_t _reserved0;
+    uint64_t seed;                /* 123 in the reference (include/RandomFunctions.cuh:21) */
+} gell_params;
+
+/*
+ * One diffusing substrate.  The reference hard-wires oxygen: boundary and uptake come from
+ * O2_Default_Concentration / Tumor_O2_consumption (include/LODkernel.cuh:41-49,80-88,100-108,288,
+ * include/Cells.cuh:74-89); D and decay are the Mesh_struct constructor arguments
+ * (include/LODkernel.cuh:205).
+ */
+typedef struct gell_substrate {
+    float boundary;   /* Dirichlet value on the two outer layers of all six faces */
+    float diffusion;  /* D, um^2/min */
+    float decay;      /* lambda, 1/min */
+    float uptake;     /* per-cell rate coefficient (negative = consumption), reference: -10 */
+    float init;       /* initial field value */
+} gell_substrate;
+
+typedef struct gell_ctx gell_ctx;
+
+/* Fill *p with the reference's compile-time values (include/Definitions.h:7-47). */
+void gell_params_default(gell_params* p);
+/* Oxygen as the reference defines it (include/Definitions.h:21-24). */
+void gell_substrate_oxygen(gell_substrate* s);
+
+/* Create a context on the current CUDA device: allocates every device buffer for
+ * max_cell_num cells and the N^3 grid.  Replaces the constructors MechanicsMesh_struct()
+ * (include/FMkernel.cuh:167-172) and the RNG set-up set_random_states (include/RandomFunctions.cuh:13,
+ * Main.cu:72-74); when rng_mode is XORWOW the per-slot states are initialised here. */
+gell_status gell_create(const gell_params* params, gell_ctx** out);
+gell_status gell_destroy(gell_ctx* ctx);
+
+/* Use `stream` (a cudaStream_t) for every later call; NULL selects the context's own stream. */
+gell_status gell_set_stream(gell_ctx* ctx, void* stream);
+
+/* Add a substrate field initialised to s->init.  Replaces Mesh_struct(float, float, float)
+ * including its host LU prefactor Mesh_initialize (include/LODkernel.cuh:205-259). */
+gell_status gell_substrate_add(gell_ctx* ctx, const gell_substrate* s, int* index_out);
+
+/* Load n cells (72-byte gell_cell records) from host or device memory; replaces the
+ * GpuCell = CpuCell copy of the reference host loop (Main.cu:91-92). */
+gell_status gell_cells_import(gell_ctx* ctx, const gell_cell* cells, int n, int cells_on_device);
+/* Write the current cells to `cells` (room for `capacity` records, host or device) and the
+ * count to *n_out; replaces CpuCell = GpuCell (Main.cu:151). Synchronises when on host. */
+gell_status gell_cells_export(gell_ctx* ctx, gell_cell* cells, int capacity, int* n_out,
+                              int cells_on_device);
+/* Current cell count (the reference's host `currentnum`).  No synchronisation. */
+gell_status gell_cell_count(gell_ctx* ctx, int* n_out);
+
+/* Dense N^3 float field, x fastest (index x + y*N + z*N*N): replaces move_to_GPU / move_to_CPU
+ * (include/LODkernel.cuh:302-309). */
+gell_status gell_field_import(gell_ctx* ctx, int substrate, const float* field, int on_device);
+gell_status gell_field_export(gell_ctx* ctx, int substrate, float* field, int on_device);
+
+/* One mechanics step: Morton keys, stable sort, cell list, forces and Adams-Bashforth move.
+ * Replaces MechanicsMesh_struct::FM_update (include/FMkernel.cuh:181-202). */
+gell_status gell_fm_update(gell_ctx* ctx);
+
+/* Uptake map of every cell into substrate `substrate` (-1 = all substrates).
+ * Replaces Mesh_struct::PreLOD (include/LODkernel.cuh:270-278). */
+gell_status gell_prelod(gell_ctx* ctx, int substrate);
+
+/* `substeps` LOD substeps (boundary, implicit source, x, y and z Thomas sweeps) of substrate
+ * `substrate` (-1 = all substrates).  Replaces Mesh_struct::LODsolver (include/LODkernel.cuh:280-300),
+ * called `substeps` times. */
+gell_status gell_lod_solver(gell_ctx* ctx, int substrate, int substeps);
+
+/* Biology step, part 1: volume and Ki-67 phase update of every live cell and division of the
+ * cells that complete mitosis.  Replaces CellBirth_kernel (include/PDkernel.cuh:88-98).
+ * Daughters are appended in the order of their mothers (the reference appends them in atomic
+ * order).  Writes the new count to *n_out when n_out is not NULL (synchronises). */
+gell_status gell_cell_birth(gell_ctx* ctx, int* n_out);
+
+/* Biology step, part 2: stable removal of every cell whose sign is false.  Replaces
+ * CellDeath_kernel (include/PDkernel.cuh:100-117).  Writes the new count when n_out != NULL. */
+gell_status gell_cell_death(gell_ctx* ctx, int* n_out);
+
+/* One mechanics step and its diffusion: gell_fm_update, gell_prelod(-1) and `substeps`
+ * gell_lod_solver(-1) calls, as the reference host loop runs them (Main.cu:114-124). */
+gell_status gell_mechanics_step(gell_ctx* ctx, int substeps);
+
+/* Wait for all work queued on the context's stream. */
+gell_status gell_sync(gell_ctx* ctx);
+
+/* Debug and parity support.  Copies the named internal array to host memory `out` (room for
+ * `bytes` bytes).  GELL_DUMP_KEYS: int32[n] Morton keys of the last fm_update in sorted order
+ * (-1 for cells outside the grid, as include/FMkernel.cuh:26-33).  GELL_DUMP_PERM: int32[n]
+ * source index of each sorted position.  GELL_DUMP_SE: int32[2*N^3], the reference's
+ * Mech_Mesh_s then Mech_Mesh_e arrays (include/FMkernel.cuh:38-53) rebuilt from the cell list.
+ * GELL_DUMP_RATE: float[N^3] uptake map of substrate `arg`.  GELL_DUMP_EF: float[2*N]
+ * Thomas factors E then F of substrate `arg` (include/LODkernel.cuh:239-259). */
+enum {
+    GELL_DUMP_KEYS = 1,
+    GELL_DUMP_PERM = 2,
+    GELL_DUMP_SE = 3,
+    GELL_DUMP_RATE = 4,
+    GELL_DUMP_EF = 5
+};
+gell_status gell_debug_dump(gell_ctx* ctx, int what, int arg, void* out, size_t bytes);
+
+const char* gell_status_string(gell_status s);
+const char* gell_last_error(gell_ctx* ctx);
+int gell_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GELL_B200_GELL_H */
