@@ -1,0 +1,382 @@
+#!/usr/bin/env python
+"""Benchmark of the gell_b200 hot path on the large plain-method workload.
+
+Workload: 400^3 voxels of 10 um, two FP32 substrates (oxygen: boundary 38, D 1e5, decay 0.1,
+uptake 10/min; drug: boundary 1, D 5e4, decay 0.05, uptake 1/min), 10^6 cells on a seeded
+jittered lattice spheroid (radius ~590 um, radii N(5, 0.5) um clipped to [4, 6]).  One step is one
+mechanics step as the reference host loop runs it: FM_update, PreLOD, then 10 LOD substeps of
+both substrates.
+
+  value      cell-updates/s of whole steps (live cells x steps / device time of the steps)
+  components cell-updates/s of FM_update + PreLOD alone, voxel-updates/s of the LOD substeps
+             (voxels x substrates x substeps / LOD device time)
+  e2e        the same rate through the C ABI with host buffers: every step imports the cells
+             from pinned host memory and exports them back, copies inside the timed region
+  roofline   the kernel with the largest device time in the timed region, against HBM
+
+`--impl reference` times the CPU restatement of the reference's hot path (the oracle, OpenMP on
+the host cores) on the same workload, each step a bounded sample: one FM_update and PreLOD on
+all cells and one LOD substep, extrapolated to the step's ten substeps of both substrates.
+
+Multi-GPU: every rank runs its own replica (the path has no exchange step); value = cells of all
+ranks / max time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s + voxel-updates/s @1M cells/400³; surrogate vs plain LOD @≤1% err"
+N, LENGTH, NCELLS, SUBSTEPS, CAP = 400, 10.0, 1_000_000, 10, 2_000_000
+NSUB = 2
+WORKLOAD = ("plain method, large: 400^3 voxels at 10 um, oxygen + drug (FP32), 10^6 cells, "
+            "1 mechanics step = FM_update + PreLOD + 10 LOD substeps")
+# algorithmic bytes per voxel-update of each LOD kernel: source + x sweep reads p and the uptake
+# rate and writes p (12 B); the y and z sweeps read and write p (8 B each)
+ALGO_BYTES = {"k_sweep_x": 12.0, "k_sweep_strided(y)": 8.0, "k_sweep_strided(z)": 8.0}
+FALLBACK_HBM_GBS = 6650.0
+
+
+def config(extra=None):
+    c = {"workload": WORKLOAD, "voxels": N ** 3, "substrates": NSUB, "cells": NCELLS,
+         "substeps_per_step": SUBSTEPS, "voxel_um": LENGTH,
+         "l2": "inputs larger than L2: each field is 256 MB, 2 fields + 2 uptake maps",
+         "parallelism": "replicas"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def make_cells():
+    from gell_b200.cells import lattice_spheroid
+    return lattice_spheroid(NCELLS, N * LENGTH / 2, 0, LENGTH, N)
+
+
+def hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---------------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons while the work runs."""
+
+    FIELDS = ("index,uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.t0 = self.t1 = None
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 10:
+                continue
+            if self.uuid and p[1] != self.uuid:
+                continue
+            rows.append(p)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        sm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        mx = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[6 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max(float(r[4]) for r in rows if r[4].replace(".", "").isdigit())
+                if any(r[4].replace(".", "").isdigit() for r in rows) else None}
+
+
+# ---------------------------------------------------------------------------- GPU arm
+
+def run_gell(args, rank, world, local_rank):
+    import torch
+    import gell_b200 as gb
+
+    torch.cuda.set_device(local_rank)
+    dist = world > 1
+    if dist:
+        import torch.distributed as td
+    cells = make_cells()
+    sim = gb.Simulation(voxel_num=N, voxel_length=LENGTH, max_cell_num=CAP)
+    sim.add_substrate(gb.oxygen())
+    sim.add_substrate(gb.drug())
+    stream = torch.cuda.Stream()
+    sim.set_stream(stream)
+    sim.import_cells(cells)
+    ncell = sim.count()
+
+    def step():
+        sim.FM_update()
+        sim.PreLOD()
+        sim.LODsolver(SUBSTEPS)
+
+    for _ in range(args.warmup):
+        step()
+    sim.sync()
+
+    props = torch.cuda.get_device_properties(local_rank)
+    uuid = getattr(props, "uuid", None)
+    uuid = f"GPU-{uuid}" if uuid is not None and not str(uuid).startswith("GPU-") else uuid
+    sampler = ClockSampler(str(uuid) if uuid else None)
+    sampler.start()
+    time.sleep(0.3)
+
+    K = args.steps
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(K)]
+    sim.profile(True)
+    sim.profile_read(reset=True)
+    launches0 = sim.launch_count()
+    if dist:
+        td.barrier()
+    torch.cuda.synchronize()
+    for k in range(K):
+        ev[k][0].record(stream)
+        sim.FM_update()
+        ev[k][1].record(stream)
+        sim.PreLOD()
+        ev[k][2].record(stream)
+        sim.LODsolver(SUBSTEPS)
+        ev[k][3].record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        td.barrier()
+    launches = sim.launch_count() - launches0
+    prof = sim.profile_read(reset=True)
+    sim.profile(False)
+    sampler.stop()
+
+    t_fm = sum(ev[k][0].elapsed_time(ev[k][1]) for k in range(K))
+    t_pre = sum(ev[k][1].elapsed_time(ev[k][2]) for k in range(K))
+    t_lod = sum(ev[k][2].elapsed_time(ev[k][3]) for k in range(K))
+    t_all = ev[0][0].elapsed_time(ev[K - 1][3])
+    alive = int(sim.export_cells()["sign"].sum())
+
+    # e2e: the same steps through the C ABI with host buffers
+    import torch as _t
+    host = _t.empty(ncell * 72, dtype=_t.uint8, pin_memory=True).numpy().view(gb.CELL_DTYPE)
+    host[:] = sim.export_cells()
+    ke = max(1, min(K, 20))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        td.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(ke):
+        sim.import_cells(host)
+        step()
+        sim.export_cells(host)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_e2e = e0.elapsed_time(e1)
+
+    times = np.array([t_all, t_fm + t_pre, t_lod, t_e2e], np.float64)
+    cells_all = np.array([alive * K, alive * ke], np.float64)
+    if dist:
+        tt = torch.tensor(times, device="cuda")
+        td.all_reduce(tt, op=td.ReduceOp.MAX)
+        times = tt.cpu().numpy()
+        cc = torch.tensor(cells_all, device="cuda")
+        td.all_reduce(cc, op=td.ReduceOp.SUM)
+        cells_all = cc.cpu().numpy()
+    t_all, t_mech, t_lod, t_e2e = times
+    value = cells_all[0] / (t_all / 1e3)
+    mech_rate = cells_all[0] / (t_mech / 1e3)
+    vox_rate = world * N ** 3 * NSUB * SUBSTEPS * K / (t_lod / 1e3)
+    e2e_rate = cells_all[1] / (t_e2e / 1e3)
+
+    # roofline of the kernel with the largest device time
+    top = max(prof.items(), key=lambda kv: kv[1][1])
+    name, (nl, ms) = top
+    avg_ms = ms / nl
+    peak, peak_kind = hbm_peak()
+    algo = ALGO_BYTES.get(name)
+    roof = {"kernel": name, "bound": "hbm", "launches": nl, "avg_ms": avg_ms, "peak": peak,
+            "peak_source": f"{peak_kind} hbm_gbs", "unit": "GB/s", "traffic": None}
+    if algo is not None:
+        per_launch = algo * N ** 3 * NSUB
+        roof.update(achieved=per_launch / (avg_ms / 1e3) / 1e9, bytes_per_launch=per_launch,
+                    bytes_per_unit=algo, unit_name="voxel-update")
+        roof["frac"] = roof["achieved"] / peak
+    shares = {k: {"launches": v[0], "ms": round(v[1], 4), "share": round(v[1] / sum(x[1] for x in prof.values()), 4)}
+              for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}
+
+    line = None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": K, "warmup": args.warmup, "ms_per_step": t_all / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: seeded jittered-lattice spheroid of 10^6 cells, fields start at the boundary values",
+            "config": config(),
+            "components": {"cell_updates_per_s_fm_prelod": mech_rate, "voxel_updates_per_s_lod": vox_rate,
+                           "ms_fm_update": t_fm / K, "ms_prelod": t_pre / K, "ms_lod_10_substeps": t_lod / K},
+            "roofline": roof,
+            "kernels": shares,
+            "e2e": {"value": e2e_rate, "unit": "cell-updates/s", "steps": ke,
+                    "h2d_bytes_per_step": int(ncell * 72), "d2h_bytes_per_step": int(ncell * 72)},
+            "gpu_launches": int(launches),
+            "clocks": sampler.summary(),
+        }
+    sim.close()
+    return line
+
+
+# ---------------------------------------------------------------------------- CPU (oracle) leg
+
+class CpuWork:
+    """The oracle (C, OpenMP) on the same workload: FM_update + PreLOD on all cells and one LOD
+    substep of one substrate per sample; substep time extrapolated to 10 substeps x 2 substrates."""
+
+    def __init__(self):
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_lib as ol
+        self.ol = ol
+        self.P = ol.params(N=N, len=LENGTH, cap=CAP)
+        self.cells = make_cells()
+        self.subs = [(38.0, 1e5, 0.1, -10.0), (1.0, 5e4, 0.05, -1.0)]
+        self.EF = [ol.mesh_init(N, LENGTH, D, dec, 0.01) for (_, D, dec, _) in self.subs]
+        self.field = [np.full(N ** 3, b, np.float32) for (b, _, _, _) in self.subs]
+        self.k = 0
+
+    def cores(self):
+        return self.ol.lib().go_get_threads()
+
+    def sample(self):
+        ol = self.ol
+        t0 = time.perf_counter()
+        ol.fm_update(self.cells, self.P)
+        t1 = time.perf_counter()
+        rates = [ol.prelod(self.cells, N, LENGTH, coef) for (_, _, _, coef) in self.subs]
+        t2 = time.perf_counter()
+        s = self.k % NSUB
+        E, F = self.EF[s]
+        L = ol.lib()
+        L.go_lod_substep(self.field[s].ctypes.data, rates[s].ctypes.data, E.ctypes.data, F.ctypes.data,
+                         N, 0.01, self.subs[s][0])
+        t3 = time.perf_counter()
+        self.k += 1
+        alive = int(self.cells["sign"].sum())
+        return alive, t1 - t0, t2 - t1, t3 - t2
+
+    def rates(self, samples):
+        fm = np.mean([s[1] for s in samples])
+        pre = np.mean([s[2] for s in samples])
+        lod = np.mean([s[3] for s in samples])
+        alive = samples[-1][0]
+        step = fm + pre + SUBSTEPS * NSUB * lod
+        return {"value": alive / step, "step_s": step, "fm_s": fm, "prelod_s": pre, "lod_substep_s": lod,
+                "mech_rate": alive / (fm + pre), "vox_rate": N ** 3 / lod}
+
+
+def cpu_baseline(n_samples=3):
+    w = CpuWork()
+    samples = [w.sample() for _ in range(n_samples)]
+    r = w.rates(samples)
+    return {"value": r["value"], "unit": "cell-updates/s", "cores": w.cores(), "kind": "port",
+            "sample": (f"{n_samples} samples of FM_update + PreLOD on all 10^6 cells and one 400^3 LOD "
+                       f"substep; step time = FM + PreLOD + 20 x substep ({r['step_s']:.2f} s)"),
+            "voxel_updates_per_s": r["vox_rate"], "cell_updates_per_s_fm_prelod": r["mech_rate"]}
+
+
+def run_reference(args):
+    w = CpuWork()
+    for _ in range(args.warmup):
+        w.sample()
+    samples = [w.sample() for _ in range(args.steps)]
+    r = w.rates(samples)
+    base = {"value": r["value"], "unit": "cell-updates/s", "cores": w.cores(), "kind": "port",
+            "sample": ("each step: FM_update + PreLOD on all 10^6 cells and one 400^3 LOD substep of one "
+                       "substrate (alternating); step time = FM + PreLOD + 20 x substep")}
+    return {
+        "impl": "reference", "metric": METRIC, "value": r["value"], "unit": "cell-updates/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["step_s"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded jittered-lattice spheroid of 10^6 cells, fields start at the boundary values",
+        "config": config({"parallelism": "host cores (rank 0 only)"}),
+        "components": {"cell_updates_per_s_fm_prelod": r["mech_rate"], "voxel_updates_per_s_lod": r["vox_rate"]},
+        "cpu_baseline": base,
+        "e2e": {"value": r["value"], "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+# ---------------------------------------------------------------------------- main
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("gell", "reference"), default="gell")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as td
+        torch.cuda.set_device(local_rank)
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    line = run_gell(args, rank, world, local_rank)
+    if rank == 0:
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline()
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as td
+        td.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

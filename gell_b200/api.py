@@ -1,0 +1,318 @@
+"""Python mirror of the gell_b200 C ABI (include/gell.h).
+
+The reference drives its hot path from a C++ host loop through member functions of
+MechanicsMesh_struct and Mesh_struct and two free functions (include/FMkernel.cuh:181,
+include/LODkernel.cuh:270,280, include/PDkernel.cuh:88,100).  `Simulation` exposes the same
+operations under the same names (FM_update, PreLOD, LODsolver, CellBirth_kernel,
+CellDeath_kernel) on top of the C ABI, for tests, benchmarks and Python callers; C and C++ callers
+use include/gell.h or include/gell_compat.hpp directly.
+
+The compute path is the CUDA library gell_b200/libgell_b200.so; there is no other implementation,
+and constructing a Simulation fails loudly when that library is missing or no GPU is visible.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+from .cells import CELL_DTYPE
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "libgell_b200.so")
+
+GELL_OK = 0
+STATUS_NAMES = {
+    0: "GELL_OK", -1: "GELL_ERR_INVALID_ARG", -2: "GELL_ERR_CAPACITY", -3: "GELL_ERR_CUDA",
+    -4: "GELL_ERR_NO_DEVICE", -5: "GELL_ERR_TIMEOUT", -6: "GELL_ERR_STATE",
+    -7: "GELL_ERR_UNSUPPORTED", -8: "GELL_ERR_ALLOC",
+}
+GELL_RNG_XORWOW, GELL_RNG_PHILOX = 0, 1
+GELL_DUMP_KEYS, GELL_DUMP_PERM, GELL_DUMP_SE, GELL_DUMP_RATE, GELL_DUMP_EF = 1, 2, 3, 4, 5
+
+F = ctypes.c_float
+D = ctypes.c_double
+I32 = ctypes.c_int32
+P = ctypes.c_void_p
+
+
+class GellParams(ctypes.Structure):
+    """struct gell_params (include/gell.h)."""
+    _fields_ = [
+        ("voxel_num", I32), ("voxel_length", F), ("max_cell_num", I32),
+        ("mechanics_dt", F), ("diffusion_dt", F), ("biology_dt", F),
+        ("ccca", F), ("cccr", F), ("ra_ratio", D), ("cc_max_dist", F),
+        ("dead_uptake_factor", F), ("default_v", F),
+        ("o2_prolif_thres", F), ("o2_prolif_sat", F), ("o2_necrosis_thres", F),
+        ("o2_necrosis_max", F),
+        ("necrosis_rate", D), ("apoptosis_rate", D), ("proliferation_rate", D),
+        ("duration_pre2post", F), ("duration_post2q", F),
+        ("o2_substrate", I32), ("rng_mode", I32), ("mech_mode", I32), ("_reserved0", I32),
+        ("seed", ctypes.c_uint64),
+    ]
+
+
+class GellProfileRecord(ctypes.Structure):
+    """struct gell_profile_record (include/gell.h)."""
+    _fields_ = [("name", ctypes.c_char * 40), ("launches", ctypes.c_int32), ("total_ms", ctypes.c_float)]
+
+
+class GellSubstrate(ctypes.Structure):
+    """struct gell_substrate (include/gell.h)."""
+    _fields_ = [("boundary", F), ("diffusion", F), ("decay", F), ("uptake", F), ("init", F)]
+
+
+@dataclass
+class Substrate:
+    boundary: float
+    diffusion: float
+    decay: float
+    uptake: float
+    init: float
+
+
+def oxygen() -> Substrate:
+    """Oxygen as the reference defines it (include/Definitions.h:21-24)."""
+    return Substrate(boundary=38.0, diffusion=1e5, decay=0.1, uptake=-10.0, init=38.0)
+
+
+def drug() -> Substrate:
+    """The second substrate of the large plain-method workload: D 5e4, decay 0.05, boundary 1,
+    uptake 1 per min; starts at its boundary value like oxygen does."""
+    return Substrate(boundary=1.0, diffusion=5e4, decay=0.05, uptake=-1.0, init=1.0)
+
+
+class GellError(RuntimeError):
+    def __init__(self, status: int, what: str, detail: str = ""):
+        self.status = status
+        super().__init__(f"{what}: {STATUS_NAMES.get(status, status)}" + (f" ({detail})" if detail else ""))
+
+
+_lib = None
+
+
+def load_library() -> ctypes.CDLL:
+    """Load gell_b200/libgell_b200.so (built by `make -C gell_b200/csrc`)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C gell_b200/csrc` "
+                          "(the CUDA library is the only implementation of the hot path)")
+    L = ctypes.CDLL(LIB_PATH)
+    L.gell_params_default.argtypes = [P]
+    L.gell_params_default.restype = None
+    L.gell_substrate_oxygen.argtypes = [P]
+    L.gell_substrate_oxygen.restype = None
+    L.gell_create.argtypes = [P, P]
+    L.gell_destroy.argtypes = [P]
+    L.gell_set_stream.argtypes = [P, P]
+    L.gell_substrate_add.argtypes = [P, P, P]
+    L.gell_cells_import.argtypes = [P, P, ctypes.c_int, ctypes.c_int]
+    L.gell_cells_export.argtypes = [P, P, ctypes.c_int, P, ctypes.c_int]
+    L.gell_cell_count.argtypes = [P, P]
+    L.gell_field_import.argtypes = [P, ctypes.c_int, P, ctypes.c_int]
+    L.gell_field_export.argtypes = [P, ctypes.c_int, P, ctypes.c_int]
+    L.gell_fm_update.argtypes = [P]
+    L.gell_prelod.argtypes = [P, ctypes.c_int]
+    L.gell_lod_solver.argtypes = [P, ctypes.c_int, ctypes.c_int]
+    L.gell_cell_birth.argtypes = [P, P]
+    L.gell_cell_death.argtypes = [P, P]
+    L.gell_mechanics_step.argtypes = [P, ctypes.c_int]
+    L.gell_sync.argtypes = [P]
+    L.gell_debug_dump.argtypes = [P, ctypes.c_int, ctypes.c_int, P, ctypes.c_size_t]
+    L.gell_status_string.argtypes = [ctypes.c_int]
+    L.gell_status_string.restype = ctypes.c_char_p
+    L.gell_last_error.argtypes = [P]
+    L.gell_last_error.restype = ctypes.c_char_p
+    L.gell_abi_version.restype = ctypes.c_int
+    L.gell_profile_enable.argtypes = [P, ctypes.c_int]
+    L.gell_profile_read.argtypes = [P, P, ctypes.c_int, P, ctypes.c_int]
+    L.gell_launch_count.argtypes = [P, P]
+    for name in ("gell_create", "gell_destroy", "gell_set_stream", "gell_substrate_add",
+                 "gell_cells_import", "gell_cells_export", "gell_cell_count", "gell_field_import",
+                 "gell_field_export", "gell_fm_update", "gell_prelod", "gell_lod_solver",
+                 "gell_cell_birth", "gell_cell_death", "gell_mechanics_step", "gell_sync",
+                 "gell_debug_dump", "gell_profile_enable", "gell_profile_read", "gell_launch_count"):
+        getattr(L, name).restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def default_params(**overrides) -> GellParams:
+    """The reference's compile-time parameter set (include/Definitions.h), with overrides."""
+    p = GellParams()
+    load_library().gell_params_default(ctypes.byref(p))
+    for k, v in overrides.items():
+        if not hasattr(p, k):
+            raise AttributeError(f"gell_params has no field {k}")
+        setattr(p, k, v)
+    return p
+
+
+def _ptr(a) -> int:
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("array must be C-contiguous")
+        return a.ctypes.data
+    return int(a.data_ptr())  # torch tensor
+
+
+class Simulation:
+    """One gell context: cells, substrates and the hot path on the current CUDA device."""
+
+    def __init__(self, params: GellParams | None = None, **overrides):
+        self.lib = load_library()
+        self.params = params if params is not None else default_params(**overrides)
+        h = P()
+        self._check(self.lib.gell_create(ctypes.byref(self.params), ctypes.byref(h)), "gell_create", None)
+        self.h = h
+        self.N = self.params.voxel_num
+        self.nsub = 0
+
+    # -- plumbing
+    def _check(self, st: int, what: str, h=-1):
+        if st != GELL_OK:
+            handle = self.h if h == -1 else h
+            detail = self.lib.gell_last_error(handle).decode() if handle else ""
+            raise GellError(st, what, detail)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.gell_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_stream(self, stream) -> None:
+        """Use a torch.cuda.Stream (or raw cudaStream_t int) for every later call."""
+        raw = getattr(stream, "cuda_stream", stream)
+        self._check(self.lib.gell_set_stream(self.h, P(raw)), "gell_set_stream")
+
+    def sync(self) -> None:
+        self._check(self.lib.gell_sync(self.h), "gell_sync")
+
+    # -- state
+    def add_substrate(self, s: Substrate) -> int:
+        c = GellSubstrate(s.boundary, s.diffusion, s.decay, s.uptake, s.init)
+        idx = ctypes.c_int()
+        self._check(self.lib.gell_substrate_add(self.h, ctypes.byref(c), ctypes.byref(idx)),
+                    "gell_substrate_add")
+        self.nsub += 1
+        return idx.value
+
+    def import_cells(self, cells, on_device: bool = False) -> None:
+        n = len(cells) if isinstance(cells, np.ndarray) else cells.shape[0] // CELL_DTYPE.itemsize
+        if isinstance(cells, np.ndarray) and cells.dtype != CELL_DTYPE:
+            raise TypeError("cells must have gell_b200.CELL_DTYPE")
+        self._check(self.lib.gell_cells_import(self.h, P(_ptr(cells) if n else 0), n, int(on_device)),
+                    "gell_cells_import")
+
+    def export_cells(self, out: np.ndarray | None = None) -> np.ndarray:
+        n = self.count()
+        if out is None:
+            out = np.zeros(max(n, 1), CELL_DTYPE)
+        cnt = ctypes.c_int()
+        self._check(self.lib.gell_cells_export(self.h, P(_ptr(out)), len(out), ctypes.byref(cnt), 0),
+                    "gell_cells_export")
+        return out[:cnt.value]
+
+    def export_cells_device(self, out_tensor) -> int:
+        """Write the cells as 72-byte records into a CUDA uint8 tensor; returns the count."""
+        cnt = ctypes.c_int()
+        cap = out_tensor.numel() // CELL_DTYPE.itemsize
+        self._check(self.lib.gell_cells_export(self.h, P(_ptr(out_tensor)), cap, ctypes.byref(cnt), 1),
+                    "gell_cells_export")
+        return cnt.value
+
+    def count(self) -> int:
+        n = ctypes.c_int()
+        self._check(self.lib.gell_cell_count(self.h, ctypes.byref(n)), "gell_cell_count")
+        return n.value
+
+    def set_field(self, sub: int, field: np.ndarray) -> None:
+        f = np.ascontiguousarray(field, np.float32).reshape(-1)
+        if f.size != self.N ** 3:
+            raise ValueError("field must hold N^3 values")
+        self._check(self.lib.gell_field_import(self.h, sub, P(f.ctypes.data), 0), "gell_field_import")
+
+    def field(self, sub: int) -> np.ndarray:
+        out = np.zeros(self.N ** 3, np.float32)
+        self._check(self.lib.gell_field_export(self.h, sub, P(out.ctypes.data), 0), "gell_field_export")
+        return out
+
+    # -- the reference's entry points
+    def FM_update(self) -> None:
+        self._check(self.lib.gell_fm_update(self.h), "gell_fm_update")
+
+    def PreLOD(self, sub: int = -1) -> None:
+        self._check(self.lib.gell_prelod(self.h, sub), "gell_prelod")
+
+    def LODsolver(self, substeps: int = 1, sub: int = -1) -> None:
+        self._check(self.lib.gell_lod_solver(self.h, sub, substeps), "gell_lod_solver")
+
+    def CellBirth_kernel(self) -> int:
+        n = ctypes.c_int()
+        self._check(self.lib.gell_cell_birth(self.h, ctypes.byref(n)), "gell_cell_birth")
+        return n.value
+
+    def CellDeath_kernel(self) -> int:
+        n = ctypes.c_int()
+        self._check(self.lib.gell_cell_death(self.h, ctypes.byref(n)), "gell_cell_death")
+        return n.value
+
+    def mechanics_step(self, substeps: int = 10) -> None:
+        self._check(self.lib.gell_mechanics_step(self.h, substeps), "gell_mechanics_step")
+
+    # -- profiling
+    def profile(self, on: bool = True) -> None:
+        self._check(self.lib.gell_profile_enable(self.h, int(on)), "gell_profile_enable")
+
+    def profile_read(self, reset: bool = True) -> dict[str, tuple[int, float]]:
+        """{kernel: (launches, total device ms)} since the last reset (synchronises)."""
+        recs = (GellProfileRecord * 64)()
+        cnt = ctypes.c_int()
+        self._check(self.lib.gell_profile_read(self.h, recs, 64, ctypes.byref(cnt), int(reset)),
+                    "gell_profile_read")
+        return {recs[i].name.decode(): (recs[i].launches, recs[i].total_ms) for i in range(cnt.value)}
+
+    def launch_count(self) -> int:
+        v = ctypes.c_int64()
+        self._check(self.lib.gell_launch_count(self.h, ctypes.byref(v)), "gell_launch_count")
+        return v.value
+
+    # -- parity support
+    def _dump(self, what: int, arg: int, dtype, count: int) -> np.ndarray:
+        out = np.zeros(max(count, 1), dtype)
+        self._check(self.lib.gell_debug_dump(self.h, what, arg, P(out.ctypes.data), out.nbytes),
+                    "gell_debug_dump")
+        return out[:count]
+
+    def dump_keys(self) -> np.ndarray:
+        return self._dump(GELL_DUMP_KEYS, 0, np.int32, self.count())
+
+    def dump_perm(self) -> np.ndarray:
+        return self._dump(GELL_DUMP_PERM, 0, np.int32, self.count())
+
+    def dump_se(self) -> tuple[np.ndarray, np.ndarray]:
+        se = self._dump(GELL_DUMP_SE, 0, np.int32, 2 * self.N ** 3)
+        return se[:self.N ** 3], se[self.N ** 3:]
+
+    def dump_rate(self, sub: int) -> np.ndarray:
+        return self._dump(GELL_DUMP_RATE, sub, np.float32, self.N ** 3)
+
+    def dump_ef(self, sub: int) -> tuple[np.ndarray, np.ndarray]:
+        ef = self._dump(GELL_DUMP_EF, sub, np.float32, 2 * self.N)
+        return ef[:self.N], ef[self.N:]

@@ -207,6 +207,21 @@ enum {
 };
 gell_status gell_debug_dump(gell_ctx* ctx, int what, int arg, void* out, size_t bytes);
 
+/* Per-kernel timing.  When enabled, every kernel this library launches is bracketed by CUDA events
+ * on the context's stream; gell_profile_read synchronises and reports, per kernel name, the number
+ * of launches and their summed device time since the last reset (replaces the host clock() timing
+ * of the reference host loop, Main.cu:101-133).  Off by default. */
+typedef struct gell_profile_record {
+    char name[40];
+    int32_t launches;
+    float total_ms;
+} gell_profile_record;
+gell_status gell_profile_enable(gell_ctx* ctx, int on);
+gell_status gell_profile_read(gell_ctx* ctx, gell_profile_record* out, int max_records, int* count,
+                              int reset);
+/* Number of kernels this context has launched (always counted). */
+gell_status gell_launch_count(gell_ctx* ctx, int64_t* count);
+
 const char* gell_status_string(gell_status s);
 const char* gell_last_error(gell_ctx* ctx);
 int gell_abi_version(void);
