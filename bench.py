@@ -43,7 +43,7 @@ WORKLOAD = ("plain method, large: 400^3 voxels at 10 um, oxygen + drug (FP32), 1
             "1 mechanics step = FM_update + PreLOD + 10 LOD substeps")
 # algorithmic bytes per voxel-update of each LOD kernel: source + x sweep reads p and the uptake
 # rate and writes p (12 B); the y and z sweeps read and write p (8 B each)
-ALGO_BYTES = {"k_sweep_x": 12.0, "k_sweep_strided(y)": 8.0, "k_sweep_strided(z)": 8.0}
+ALGO_BYTES = {"k_sweep_x": 12.0, "k_sweep_y": 8.0, "k_sweep_z": 8.0}
 FALLBACK_HBM_GBS = 6650.0
 
 

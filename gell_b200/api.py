@@ -131,11 +131,13 @@ def load_library() -> ctypes.CDLL:
     L.gell_profile_enable.argtypes = [P, ctypes.c_int]
     L.gell_profile_read.argtypes = [P, P, ctypes.c_int, P, ctypes.c_int]
     L.gell_launch_count.argtypes = [P, P]
+    L.gell_selftest_division.argtypes = [P, ctypes.c_int64, ctypes.c_uint64, P]
     for name in ("gell_create", "gell_destroy", "gell_set_stream", "gell_substrate_add",
                  "gell_cells_import", "gell_cells_export", "gell_cell_count", "gell_field_import",
                  "gell_field_export", "gell_fm_update", "gell_prelod", "gell_lod_solver",
                  "gell_cell_birth", "gell_cell_death", "gell_mechanics_step", "gell_sync",
-                 "gell_debug_dump", "gell_profile_enable", "gell_profile_read", "gell_launch_count"):
+                 "gell_debug_dump", "gell_profile_enable", "gell_profile_read", "gell_launch_count",
+                 "gell_selftest_division"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
@@ -287,6 +289,13 @@ class Simulation:
         self._check(self.lib.gell_profile_read(self.h, recs, 64, ctypes.byref(cnt), int(reset)),
                     "gell_profile_read")
         return {recs[i].name.decode(): (recs[i].launches, recs[i].total_ms) for i in range(cnt.value)}
+
+    def selftest_division(self, samples: int, seed: int = 1) -> int:
+        """Mismatches of the sweeps' division against IEEE division over random operands."""
+        m = ctypes.c_int64()
+        self._check(self.lib.gell_selftest_division(self.h, samples, seed, ctypes.byref(m)),
+                    "gell_selftest_division")
+        return m.value
 
     def launch_count(self) -> int:
         v = ctypes.c_int64()

@@ -1,7 +1,9 @@
 // ctx.cu — C ABI of gell_b200 (include/gell.h): context lifetime, cell and field import/export,
 // and debug dumps.  The compute entry points live in lod.cu, mech.cu and pd.cu.
+#include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <cudaTypedefs.h>
 #include <new>
 
 #include "gell_internal.cuh"
@@ -184,7 +186,7 @@ static void free_all(gell_ctx* c) {
     }
     f(c->sort.hist);
     f(c->bins);
-    for (auto& s : c->subs) { f(s.p); f(s.rate); f(s.EF); f(s.line_flag); f(s.line_list); f(s.line_count); }
+    for (auto& s : c->subs) { f(s.p); f(s.rate); f(s.EF); f(s.FRS); f(s.line_flag); f(s.line_list); f(s.line_count); }
     f(c->xorwow); f(c->flags); f(c->scan_tmp); f(c->dev_count); f(c->dev_err);
     f(c->staging);
     for (auto& p : c->prof) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
@@ -321,6 +323,52 @@ static void mesh_init(int N, float len, float D, float decay, float dt, std::vec
     F[N - 1] = corner - E[N - 1] * side;
 }
 
+// RN(1/f): the float nearest to 1/f.  The product of two floats is exact in double, so
+// |1 - y*f| ranks the candidates exactly; 1/f of a float is never halfway between two floats.
+static float recip_rn(float f) {
+    const float y0 = (float)(1.0 / (double)f);
+    float best = y0;
+    double berr = fabs(1.0 - (double)y0 * (double)f);
+    const float cand[2] = {nextafterf(y0, -INFINITY), nextafterf(y0, INFINITY)};
+    for (float y : cand) {
+        const double e = fabs(1.0 - (double)y * (double)f);
+        if (e < berr) { best = y; berr = e; }
+    }
+    return best;
+}
+
+// TMA maps of a pitched field: x boxes [32 lines][32 elements] with the 128-byte swizzle over
+// (P, N*N); y boxes [32 elements][32 lines] over (P, N, N); z boxes over (P*N, N).
+static gell_status make_tensor_maps(gell_ctx* c, Substrate& sub) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        cudaDriverEntryPointQueryResult q;
+        void* fn = nullptr;
+        cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+            return fail(c, GELL_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+        encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    const cuuint64_t N = (cuuint64_t)c->g.N, P = (cuuint64_t)c->g.P;
+    const cuuint32_t box2[2] = {32, 32}, box3[3] = {32, 32, 1}, es[3] = {1, 1, 1};
+    const cuuint64_t dx[2] = {P, N * N}, sx[1] = {P * 4};
+    const cuuint64_t dy[3] = {P, N, N}, sy[2] = {P * 4, P * N * 4};
+    const cuuint64_t dz[2] = {P * N, N}, sz[1] = {P * N * 4};
+    CUresult r = encode(&sub.tmap[0], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, sub.p, dx, sx, box2, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r == CUDA_SUCCESS)
+        r = encode(&sub.tmap[1], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, sub.p, dy, sy, box3, es,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r == CUDA_SUCCESS)
+        r = encode(&sub.tmap[2], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, sub.p, dz, sz, box2, es,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(c, GELL_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return GELL_OK;
+}
+
 gell_status gell_substrate_add(gell_ctx* c, const gell_substrate* s, int* index_out) {
     if (!c || !s) return GELL_ERR_INVALID_ARG;
     if (c->subs.size() >= 8) return fail(c, GELL_ERR_UNSUPPORTED, "at most 8 substrates");
@@ -332,7 +380,7 @@ gell_status gell_substrate_add(gell_ctx* c, const gell_substrate* s, int* index_
     size_t nl = (size_t)c->g.N * c->g.N;
     cudaError_t e = cudaMalloc(&sub.p, fb);
     if (e == cudaSuccess) e = cudaMalloc(&sub.rate, fb);
-    if (e == cudaSuccess) e = cudaMalloc(&sub.EF, (size_t)c->g.N * 2 * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&sub.EF, (size_t)c->g.N * 3 * 4);
     if (e == cudaSuccess) e = cudaMalloc(&sub.line_flag, nl * 4);
     if (e == cudaSuccess) e = cudaMalloc(&sub.line_list, nl * 4);
     if (e == cudaSuccess) e = cudaMalloc(&sub.line_count, 4);
@@ -344,8 +392,33 @@ gell_status gell_substrate_add(gell_ctx* c, const gell_substrate* s, int* index_
     }
     GELL_CUDA(c, cudaMemsetAsync(sub.line_flag, 0, nl * 4, c->stream));
     GELL_CUDA(c, cudaMemsetAsync(sub.line_count, 0, 4, c->stream));
-    GELL_CUDA(c, cudaMemcpyAsync(sub.EF, sub.E.data(), c->g.N * 4, cudaMemcpyHostToDevice, c->stream));
-    GELL_CUDA(c, cudaMemcpyAsync(sub.EF + c->g.N, sub.F.data(), c->g.N * 4, cudaMemcpyHostToDevice, c->stream));
+    {
+        gell_status ts = make_tensor_maps(c, sub);
+        if (ts != GELL_OK) {
+            for (void* q : {(void*)sub.p, (void*)sub.rate, (void*)sub.EF, (void*)sub.line_flag,
+                            (void*)sub.line_list, (void*)sub.line_count})
+                cudaFree(q);
+            return ts;
+        }
+    }
+    // device table: E, F and RN(1/F) for the division on the back-substitution chain
+    std::vector<float> efr(3 * (size_t)c->g.N);
+    for (int i = 0; i < c->g.N; ++i) {
+        efr[i] = sub.E[i];
+        efr[c->g.N + i] = sub.F[i];
+        efr[2 * c->g.N + i] = recip_rn(sub.F[i]);
+    }
+    GELL_CUDA(c, cudaMemcpy(sub.EF, efr.data(), efr.size() * 4, cudaMemcpyHostToDevice));
+    {
+        const int Na = (c->g.N + 31) / 32 * 32;
+        std::vector<float4> frs((size_t)Na);
+        for (int j = 0; j < Na; ++j) {
+            const bool in = j >= 1 && j <= c->g.N - 2;
+            frs[j] = in ? make_float4(sub.F[j], efr[2 * c->g.N + j], sub.side, 0.f) : make_float4(1.f, 1.f, 0.f, 0.f);
+        }
+        GELL_CUDA(c, cudaMalloc(&sub.FRS, frs.size() * sizeof(float4)));
+        GELL_CUDA(c, cudaMemcpy(sub.FRS, frs.data(), frs.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    }
     GELL_KERNEL(c, "k_fill", k_fill<<<blocks_for(c->nvox_p, 256), 256, 0, c->stream>>>(sub.p, c->nvox_p, s->init));
     GELL_CUDA(c, cudaMemsetAsync(sub.rate, 0, fb, c->stream));
     // the new map must cover the current cells before the next LOD substep
@@ -464,6 +537,14 @@ gell_status gell_profile_read(gell_ctx* c, gell_profile_record* out, int max_rec
         c->prof.clear();
     }
     return GELL_OK;
+}
+
+gell_status gell_selftest_division(gell_ctx* c, int64_t samples, uint64_t seed, int64_t* mismatches) {
+    if (!c || !mismatches || samples < 0) return GELL_ERR_INVALID_ARG;
+    long long m = 0;
+    gell_status st = selftest_division(c, samples, seed, &m);
+    *mismatches = m;
+    return st;
 }
 
 gell_status gell_launch_count(gell_ctx* c, int64_t* count) {

@@ -13,6 +13,7 @@
 //            them: the uptake map is zero elsewhere and only listed lines are read or cleared
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <curand_kernel.h>
 #include <stdint.h>
@@ -52,12 +53,15 @@ struct Substrate {
     gell_substrate s;
     float* p = nullptr;     // field, pitched
     float* rate = nullptr;  // uptake map, pitched; nonzero only on flagged lines
-    float* EF = nullptr;    // device: E[N], F[N]
+    float* EF = nullptr;    // device: E[N], F[N], RN(1/F)[N]
+    float4* FRS = nullptr;  // device: (F, RN(1/F), s, 0) per element of 32*ceil(N/32), boundary
+                            // elements (0 and >= N-1) as identities (1, 1, 0, 0)
     uint32_t* line_flag = nullptr;  // N*N: x-line (y + z*N) holds uptake
     int* line_list = nullptr;       // flagged lines
     int* line_count = nullptr;      // device: number of flagged lines
     std::vector<float> E, F;
     float side = 0.f;       // E[1]*F[0], the sweeps' off-diagonal (thomas_side)
+    CUtensorMap tmap[3];    // TMA maps of the field for the x, y and z sweeps (32x32 boxes)
 };
 
 // Kernel-side view of the geometry.
@@ -227,6 +231,7 @@ gell_status scan_u32(gell_ctx* c, const uint32_t* in, uint32_t* out, int n, int*
 // stable LSD radix sort of (keys, vals) over the low `bits` bits; result in c->sort.which
 gell_status radix_sort(gell_ctx* c, int n, int bits, bool vals_are_iota);
 gell_status dump_se(gell_ctx* c, int* host_out);
+gell_status selftest_division(gell_ctx* c, long long n, unsigned long long seed, long long* mismatches);
 size_t sort_hist_entries(int cap);
 
 }  // namespace gell

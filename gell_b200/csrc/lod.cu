@@ -1,20 +1,33 @@
 // lod.cu — LOD reaction-diffusion of the substrates (include/LODkernel.cuh:12-136,183-300).
 //
 // One substep of the reference (Mesh_struct::LODsolver) is Setboundary, meshupdatekernel and the
-// three Thomas sweeps LODkernel_x/y/z, each a separate launch over one thread per line.  Here a
-// substep is three launches, all substrates in each:
-//   k_sweep_x        boundary layers + implicit uptake source + x sweep, fused per x-line
-//   k_sweep_strided  y sweep (axis 1) and z sweep (axis 2)
-// Every line is staged in shared memory by bulk asynchronous copies (the Blackwell TMA engine)
-// completing on an mbarrier; each lane then runs one line's recurrence out of shared memory.
-// x-lines are contiguous rows (one bulk copy per line, tile [32 lines][S]); y- and z-lines are
-// strided, so a tile is 32 neighbouring lines and each bulk copy moves one 128-byte row of it
-// (tile [N rows][32 lanes]), which makes every global access a full, coalesced row.
+// three Thomas sweeps LODkernel_x/y/z, each a launch of one thread per line.  Here a substep is
+// three launches of one kernel template, all substrates in each:
+//   k_sweep<0>  boundary layers + implicit uptake source + x sweep (x-lines are contiguous)
+//   k_sweep<1>  y sweep (element stride P)      k_sweep<2>  z sweep (element stride P*N)
 //
-// Arithmetic per line, identical to the reference kernels with nvcc's multiply-add fusion:
+// Streaming line tiles.  A warp owns a tile of 32 lines (one per lane) and walks its lane's line
+// out of shared memory.  The line is cut into B = ceil(N/32) groups of 32 elements; each group of
+// the tile is one 32x32 TMA tensor box (4 KB) moved by one instruction and completing on the
+// group's mbarrier, so the forward elimination starts as soon as group 0 has landed.  The back
+// substitution finishes the groups from the top down; each finished group is written back by one
+// TMA tensor store, and the slot it occupied is refilled with a group of the warp's NEXT tile.
+// Groups live in B slots of 4 KB: a tile of parity 0 keeps group g in slot g, a tile of parity 1
+// in slot B-1-g, so the slots freed first by the back substitution (top groups) are the ones the
+// next tile needs first (bottom groups).  Each warp therefore always has its next tile in flight.
+//   y/z boxes are [32 elements][32 lines] (128-byte rows, one row per element)
+//   x boxes are [32 lines][32 elements] with the 128-byte swizzle, so each lane reads four
+//       consecutive elements of its line with one conflict-free 16-byte load
+//
+// Arithmetic per line, the reference kernels' with nvcc's multiply-add fusion:
 //   Y0 = b; Y_i = fma(-E_i, Y_{i-1}, p_i) (i = 1..N-2); x_{N-1} = b;
 //   x_i = fma(-s, x_{i+1}, Y_i) / F_i (i = N-2..1); x_0 = b;  s = E[1]*F[0]
-// and the source p /= fma(-rate, dt, 1).  Division is IEEE round-to-nearest.
+// and the source p /= fma(-rate, dt, 1).  The division on the back-substitution chain is
+// Markstein's (IBM J. Res. Dev. 34(1), 1990): with y = RN(1/F_i) precomputed on the host, two
+// residual corrections q += (a - F q) y give the correctly rounded quotient, equal to IEEE
+// division (checked against it by gell_selftest_division and by the bit-exact parity tests).
+#include <cuda.h>
+
 #include "gell_internal.cuh"
 
 namespace gell {
@@ -22,19 +35,21 @@ namespace gell {
 namespace {
 
 constexpr int kMaxSub = 8;
-constexpr int kChunks = 4;  // mbarriers per strided tile, so the forward pass starts early
 constexpr unsigned FULL = 0xffffffffu;
+constexpr int kSlotFloats = 32 * 32;
 
 struct SubDev {
-    float* p;
+    float* p;          // field (pitched)
     const float* rate;
     const uint32_t* line_flag;
-    const float* EF;
+    const float* EFR;  // E[N], F[N], RN(1/F)[N]
+    const float4* FRS; // per element (F, RN(1/F), s, 0), boundary elements as identities
     float b;
     float side;
 };
 
 struct LodArgs {
+    CUtensorMap tm[kMaxSub];  // one map per substrate for this kernel's axis
     SubDev sub[kMaxSub];
     int nsub;
     Geom g;
@@ -78,222 +93,487 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, int* err
     if ((threadIdx.x & 31) == 0) atomicExch(err, code);
     return false;
 }
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* tm, int c0, int c1, uint64_t* bar) {
     asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
             smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        "l"(tm), "r"(c0), "r"(c1), "r"(smem_u32(bar))
         : "memory");
 }
-__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
-    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
-                 "r"(smem_u32(src)), "r"(bytes)
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* tm, int c0, int c1, int c2, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+            smem_u32(dst)),
+        "l"(tm), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* tm, int c0, int c1, const void* src) {
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"(tm), "r"(c0),
+                 "r"(c1), "r"(smem_u32(src))
+                 : "memory");
+}
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* tm, int c0, int c1, int c2, const void* src) {
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(tm),
+                 "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(src))
                  : "memory");
 }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read0() {
-    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+template <int K>
+__device__ __forceinline__ void bulk_wait_read() {
+    asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(K) : "memory");
 }
 
 __host__ __device__ inline int align128(int b) { return (b + 127) / 128 * 128; }
 
-// Shared-memory row stride of an x-tile: >= P, a multiple of 4 floats (16-byte rows for the bulk
-// copies) with an odd number of 16-byte units, so that 32 lanes reading float4 element c of their
-// own rows hit distinct banks.
-__host__ __device__ inline int xrow_stride(int P) { return ((P / 4) % 2 == 1) ? P : P + 4; }
+// Correctly rounded a / f given y = RN(1/f) (Markstein): q0 = a*y is within 2 ulp, one residual
+// step makes it faithful, the second rounds it correctly.  Valid away from overflow/underflow.
+__device__ __forceinline__ float div_rn(float a, float f, float y) {
+    float q = __fmul_rn(a, y);
+    float r = __fmaf_rn(-q, f, a);
+    q = __fmaf_rn(r, y, q);
+    r = __fmaf_rn(-q, f, a);
+    return __fmaf_rn(r, y, q);
+}
 
-__device__ __forceinline__ void load_ef(float* sEF, const LodArgs& a) {
-    const int N = a.g.N;
-    for (int i = threadIdx.x; i < a.nsub * 2 * N; i += blockDim.x) {
-        int s = i / (2 * N), r = i - s * 2 * N;
-        sEF[i] = a.sub[s].EF[r];
+// One tile: 32 lines of one substrate, addressed by TMA coordinates.
+struct TileDesc {
+    int s;       // substrate
+    int c0, c2;  // x: line0 (c0);  y: x0 (c0), z (c2);  z: L0 (c0)
+    bool interior_lane, flagged_lane;  // x only
+    long long line;                    // x: this lane's line (y + z*N)
+};
+
+template <int AXIS>
+__device__ __forceinline__ TileDesc tile_desc(const LodArgs& a, long long t, long long per_sub) {
+    const Geom& g = a.g;
+    const int N = g.N, P = g.P;
+    const int lane = threadIdx.x & 31;
+    TileDesc d;
+    d.s = (int)(t / per_sub);
+    const long long tt = t - d.s * per_sub;
+    d.c2 = 0;
+    d.interior_lane = d.flagged_lane = false;
+    d.line = 0;
+    if (AXIS == 0) {
+        const long long nl = (long long)N * N;
+        d.c0 = (int)(tt * 32);
+        d.line = (long long)d.c0 + lane;
+        const bool valid = d.line < nl;
+        const int y = valid ? (int)(d.line % N) : 0, z = valid ? (int)(d.line / N) : 0;
+        d.interior_lane = valid && y >= 2 && y < N - 2 && z >= 2 && z < N - 2;
+        d.flagged_lane = valid && a.sub[d.s].line_flag[d.line] != 0u;
+    } else if (AXIS == 1) {
+        const int ntx = (P + 31) / 32;
+        d.c2 = (int)(tt / ntx);
+        d.c0 = (int)(tt - (long long)d.c2 * ntx) * 32;
+    } else {
+        d.c0 = (int)(tt * 32);
+    }
+    return d;
+}
+
+// TMA box of group g of tile d: load into `slot` (completing on `bar`) or store from it.
+template <int AXIS>
+__device__ __forceinline__ void box_load(const LodArgs& a, const TileDesc& d, int g, float* slot, uint64_t* bar) {
+    mbar_arrive_expect(bar, kSlotFloats * 4);
+    if (AXIS == 0) tma_load_2d(slot, &a.tm[d.s], 32 * g, d.c0, bar);
+    else if (AXIS == 1) tma_load_3d(slot, &a.tm[d.s], d.c0, 32 * g, d.c2, bar);
+    else tma_load_2d(slot, &a.tm[d.s], d.c0, 32 * g, bar);
+}
+template <int AXIS>
+__device__ __forceinline__ void box_store(const LodArgs& a, const TileDesc& d, int g, const float* slot) {
+    if (AXIS == 0) tma_store_2d(&a.tm[d.s], 32 * g, d.c0, slot);
+    else if (AXIS == 1) tma_store_3d(&a.tm[d.s], d.c0, 32 * g, d.c2, slot);
+    else tma_store_2d(&a.tm[d.s], d.c0, 32 * g, slot);
+}
+
+// Per-element tables.  Boundary elements (j = 0 and j >= N-1) are identities: E = 0 makes
+// Y_j = p_j (= b, set by the pre-pass), and (F, 1/F, s) = (1, 1, 0) makes x_j = Y_j = b, which is
+// what the reference's x_0 = x_{N-1} = b gives (it never uses Y at N-1).  Every group therefore
+// runs the same code.
+struct SweepCtx {
+    const float* E;    // E[j] (16-byte aligned)
+    const float4* FR;  // (F[j], RN(1/F[j]), s[j], 0) (16-byte aligned)
+    float b, dt;
+};
+
+// Address of element e (0..31) of this lane's line in a slot.  x slots are [line][element] with
+// the 128-byte swizzle (16-byte chunk c of row r stored at chunk c ^ (r & 7)); y/z slots are
+// [element][line].
+template <int AXIS>
+__device__ __forceinline__ float* elem(float* slot, int e, int lane) {
+    if (AXIS == 0) return slot + lane * 32 + (((e >> 2) ^ (lane & 7)) << 2) + (e & 3);
+    return slot + e * 32 + lane;
+}
+
+// 8 consecutive elements e0..e0+7 (e0 a multiple of 8) of this lane's line.
+template <int AXIS>
+__device__ __forceinline__ void load8(float* slot, int e0, int lane, float v[8]) {
+    if (AXIS == 0) {
+        const float4 a = *reinterpret_cast<const float4*>(elem<0>(slot, e0, lane));
+        const float4 b = *reinterpret_cast<const float4*>(elem<0>(slot, e0 + 4, lane));
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+        v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = slot[(e0 + k) * 32 + lane];
+    }
+}
+template <int AXIS>
+__device__ __forceinline__ void store8(float* slot, int e0, int lane, const float v[8]) {
+    if (AXIS == 0) {
+        *reinterpret_cast<float4*>(elem<0>(slot, e0, lane)) = make_float4(v[0], v[1], v[2], v[3]);
+        *reinterpret_cast<float4*>(elem<0>(slot, e0 + 4, lane)) = make_float4(v[4], v[5], v[6], v[7]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) slot[(e0 + k) * 32 + lane] = v[k];
     }
 }
 
-// Thomas recurrence of one line held in shared memory (row), in place, float4 at a time.
-__device__ __forceinline__ void thomas_row(float* row, const float* E, const float* F, float s,
-                                           float b, int N) {
-    float4* r4 = reinterpret_cast<float4*>(row);
-    float Y = b;
-    const int cmax = (N - 2) / 4;  // last chunk holding an element <= N-2
-    for (int c = 0; c <= cmax; ++c) {
-        float4 q = r4[c];
-        float e[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            int i = 4 * c + k;
-            if (i >= 1 && i <= N - 2) {
-                Y = __fmaf_rn(-E[i], Y, e[k]);
-                e[k] = Y;
-            }
+// x: Setboundary for lines without uptake, in place on group g of the tile, one line at a time
+// across the warp (lane = element): the two outer layers of every face hold b.  Lines with uptake
+// were prepared by k_source_lines (boundary and source already applied); for them only elements 0
+// and N-1 are set, to the reference's Y_0 = b and x_{N-1} = b.
+__device__ __forceinline__ void x_prepass(const SweepCtx& c, float* slot, int g, int N, uint32_t lines,
+                                          uint32_t interior, uint32_t flagged) {
+    const int lane = threadIdx.x & 31;
+    const int j = 32 * g + lane;
+    const bool outer = j < 2 || j > N - 3;
+    const bool ends = j == 0 || j >= N - 1;
+    while (lines) {
+        const int r = __ffs(lines) - 1;
+        lines &= lines - 1;
+        float* p = slot + r * 32 + (((lane >> 2) ^ (r & 7)) << 2) + (lane & 3);
+        if ((flagged >> r) & 1u) {
+            if (ends) *p = c.b;
+        } else if (!((interior >> r) & 1u) || outer) {
+            *p = c.b;
         }
-        r4[c] = make_float4(e[0], e[1], e[2], e[3]);
     }
-    float x = b;
-    for (int c = cmax; c >= 0; --c) {
-        float4 q = r4[c];
-        float e[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-        for (int k = 3; k >= 0; --k) {
-            int i = 4 * c + k;
-            if (i >= 1 && i <= N - 2) {
-                x = __fdiv_rn(__fmaf_rn(-s, x, e[k]), F[i]);
-                e[k] = x;
-            }
-        }
-        r4[c] = make_float4(e[0], e[1], e[2], e[3]);
-    }
-    row[0] = b;
-    row[N - 1] = b;
+    __syncwarp();
 }
 
-// Boundary layers + source + x sweep.  A warp owns 32 consecutive x-lines (line = y + z*N).
-__global__ void __launch_bounds__(512) k_sweep_x(LodArgs a) {
-    extern __shared__ __align__(128) unsigned char sm[];
-    const Geom g = a.g;
-    const int N = g.N, P = g.P, S = xrow_stride(P);
-    const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float* sEF = reinterpret_cast<float*>(sm);
-    const int efb = align128(a.nsub * 2 * N * 4);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sm + efb);
-    float* tile = reinterpret_cast<float*>(sm + efb + align128(warps * 8)) + (size_t)warp * 32 * S;
-    uint64_t* bar = bars + warp;
-    load_ef(sEF, a);
-    if (lane == 0) mbar_init(bar, 1);
-    fence_mbar_init();
-    __syncthreads();
+// Forward elimination over group g: Y_j = fma(-E_j, Y_{j-1}, p_j) for the 32 elements of the group,
+// 8 at a time with the next batch's values and E already requested.
+template <int AXIS>
+__device__ __forceinline__ void forward_group(const SweepCtx& c, float* slot, int g, int lane, float& Y) {
+    const int j0 = 32 * g;
+    float v[8], w[8];
+    float4 e0 = *reinterpret_cast<const float4*>(c.E + j0);
+    float4 e1 = *reinterpret_cast<const float4*>(c.E + j0 + 4);
+    load8<AXIS>(slot, 0, lane, v);
+#pragma unroll
+    for (int b8 = 0; b8 < 4; ++b8) {
+        float4 n0 = e0, n1 = e1;
+        if (b8 < 3) {
+            load8<AXIS>(slot, 8 * b8 + 8, lane, w);
+            n0 = *reinterpret_cast<const float4*>(c.E + j0 + 8 * b8 + 8);
+            n1 = *reinterpret_cast<const float4*>(c.E + j0 + 8 * b8 + 12);
+        }
+        const float ev[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            Y = __fmaf_rn(-ev[k], Y, v[k]);
+            v[k] = Y;
+        }
+        store8<AXIS>(slot, 8 * b8, lane, v);
+        if (b8 < 3) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v[k] = w[k];
+            e0 = n0;
+            e1 = n1;
+        }
+    }
+}
 
-    const long long nlines = (long long)N * N;
-    const long long per_sub = (nlines + 31) / 32;
-    const long long total = per_sub * a.nsub;
-    uint32_t parity = 0;
-    for (long long t = (long long)blockIdx.x * warps + warp; t < total; t += (long long)gridDim.x * warps) {
-        const int s = (int)(t / per_sub);
-        const long long tt = t - s * per_sub;
-        const SubDev sd = a.sub[s];
-        const float* E = sEF + s * 2 * N;
-        const float* F = E + N;
-        const long long line = tt * 32 + lane;
-        const bool valid = line < nlines;
-        const int y = valid ? (int)(line % N) : 0, z = valid ? (int)(line / N) : 0;
-        // every voxel of a line in the two outer layers of a y or z face is set to b
-        const bool bline = !valid || y < 2 || y >= N - 2 || z < 2 || z >= N - 2;
-        float* gl = sd.p + line * P;
-        const unsigned m = __ballot_sync(FULL, !bline);
-        if (m) {
-            if (lane == 0) mbar_arrive_expect(bar, (uint32_t)__popc(m) * P * 4);
+// Back substitution step with the exact division: x = (y - s x) / F.
+__device__ __forceinline__ float back_exact(float x, float y, float f, float rf, float sd) {
+    return div_rn(__fmaf_rn(-sd, x, y), f, rf);
+}
+
+// Back substitution over a full group (elements 32g+31 .. 32g, all in [1, N-2]), results in o[].
+// The chain carries a1, the once-corrected quotient started from fma(-s/F, x, y/F); the exact
+// quotient a2 is computed beside it.  If any lane's a1 differs from its a2 anywhere in the group,
+// the whole group is recomputed on the exact chain, so o[] always holds the exact values.
+template <int AXIS>
+__device__ __forceinline__ void backward_full(const SweepCtx& c, float* slot, int j0, int lane, float& x,
+                                              float o[32]) {
+    const float x_in = x;
+    uint32_t bad = 0;
+    float v[8], w[8];
+    const float4* fb = c.FR + j0;
+    float4 f[8], h[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) f[k] = __ldg(fb + 24 + k);
+    load8<AXIS>(slot, 24, lane, v);
+#pragma unroll
+    for (int b8 = 3; b8 >= 0; --b8) {
+        if (b8 > 0) {
+            load8<AXIS>(slot, 8 * b8 - 8, lane, w);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) h[k] = __ldg(fb + 8 * b8 - 8 + k);
+        }
+        float yr[8], sr[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            yr[k] = __fmul_rn(v[k], f[k].y);
+            sr[k] = __fmul_rn(f[k].z, f[k].y);
+        }
+#pragma unroll
+        for (int k = 7; k >= 0; --k) {
+            const float t = __fmaf_rn(-f[k].z, x, v[k]);
+            const float a0 = __fmaf_rn(-sr[k], x, yr[k]);
+            const float r0 = __fmaf_rn(-a0, f[k].x, t);
+            const float a1 = __fmaf_rn(r0, f[k].y, a0);   // carried on the chain
+            const float r1 = __fmaf_rn(-a1, f[k].x, t);
+            const float a2 = __fmaf_rn(r1, f[k].y, a1);   // exact quotient of t by F
+            bad |= __float_as_uint(a1) ^ __float_as_uint(a2);
+            x = a1;
+            o[8 * b8 + k] = a1;
+        }
+        if (b8 > 0) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                v[k] = w[k];
+                f[k] = h[k];
+            }
+        }
+    }
+    if (__any_sync(FULL, bad != 0)) {
+        x = x_in;
+#pragma unroll
+        for (int e = 31; e >= 0; --e) {
+            const float4 fr = __ldg(c.FR + j0 + e);
+            x = back_exact(x, *elem<AXIS>(slot, e, lane), fr.x, fr.y, fr.z);
+            o[e] = x;
+        }
+    }
+}
+
+// Back substitution over group g, from its top element down.  x: results go back into the slot
+// (stored by TMA afterwards); y/z: results go straight to global memory from registers, a full
+// 128-byte row per element (gcol = this lane's line at element 0, es = element stride), for the
+// elements below N.
+template <int AXIS>
+__device__ __forceinline__ void backward_group(const SweepCtx& c, float* slot, int g, int N, int lane, float& x,
+                                               float* gcol, long long es, bool store_ok) {
+    const int j0 = 32 * g;
+    float o[32];
+    backward_full<AXIS>(c, slot, j0, lane, x, o);
+    if (AXIS == 0) {
+#pragma unroll
+        for (int b8 = 0; b8 < 4; ++b8) store8<AXIS>(slot, 8 * b8, lane, o + 8 * b8);
+    } else if (store_ok) {
+        const int ne = min(32, N - j0);
+        float* gp = gcol + (long long)j0 * es;
+        if (ne == 32) {
+#pragma unroll
+            for (int e = 0; e < 32; ++e) {
+                gp[0] = o[e];
+                gp += es;
+            }
+        } else {
+#pragma unroll
+            for (int e = 0; e < 32; ++e) {
+                if (e < ne) gp[0] = o[e];
+                gp += es;
+            }
+        }
+    }
+}
+
+// y/z: rows of the end groups that hold boundary elements (j = 0 and j >= N-1) get b.
+template <int AXIS>
+__device__ __forceinline__ void edge_rows(const SweepCtx& c, float* slot, int g, int N, int lane) {
+    const int j0 = 32 * g;
+    if (g == 0) slot[lane] = c.b;
+    for (int e = max(N - 1 - j0, 0); e < 32; ++e) slot[e * 32 + lane] = c.b;
+    __syncwarp();
+}
+
+// One tile of parity Q: forward elimination as its groups land, back substitution from the top
+// group down, every finished group stored by TMA and its slot refilled with the next tile.
+template <int AXIS, int Q>
+__device__ __forceinline__ bool run_tile(const LodArgs& a, const TileDesc& d, const TileDesc& dn, bool has_next,
+                                         float* buf, uint64_t* bars, uint32_t& ph, const float* sEFR, int Na) {
+    const int N = a.g.N, P = a.g.P;
+    const int B = (N + 31) >> 5;
+    const int lane = threadIdx.x & 31;
+    const SubDev& sd = a.sub[d.s];
+    SweepCtx c;
+    c.E = sEFR + (size_t)d.s * Na;
+    c.FR = sd.FRS;
+    c.b = sd.b;
+    c.dt = a.dt;
+    auto slot_of = [&](int g, int q) { return buf + (size_t)(q ? B - 1 - g : g) * kSlotFloats; };
+    uint32_t interior = 0, flagged = 0, special = 0;
+    if (AXIS == 0) {
+        interior = __ballot_sync(FULL, d.interior_lane);
+        flagged = __ballot_sync(FULL, d.flagged_lane);
+        special = ~interior & ~flagged;  // boundary lines: every group needs the reset
+    }
+
+    float Y = c.b;
+    for (int g = 0; g < B; ++g) {
+        if (!mbar_wait(bars + g, (ph >> g) & 1u, a.err, 1 + AXIS)) return false;
+        ph ^= 1u << g;
+        float* slot = slot_of(g, Q);
+        const bool edge = g == 0 || 32 * g + 31 > N - 3;
+        if (AXIS == 0) {
+            const uint32_t lines = edge ? 0xffffffffu : special;
+            if (lines) x_prepass(c, slot, g, N, lines, interior, flagged);
+        } else if (edge) {
+            edge_rows<AXIS>(c, slot, g, N, lane);
+        }
+        forward_group<AXIS>(c, slot, g, lane, Y);
+    }
+    float x = c.b;
+    // this lane's column in global memory (y/z): element 0 of its line, and the element stride
+    float* gcol = nullptr;
+    long long es = 0;
+    bool store_ok = false;
+    if (AXIS == 1) {
+        gcol = sd.p + d.c0 + lane + (long long)d.c2 * a.g.PN;
+        es = P;
+        store_ok = d.c0 + lane < P;
+    } else if (AXIS == 2) {
+        gcol = sd.p + d.c0 + lane;
+        es = a.g.PN;
+        store_ok = d.c0 + lane < a.g.PN;
+    }
+    for (int g = B - 1; g >= 0; --g) {
+        float* slot = slot_of(g, Q);
+        backward_group<AXIS>(c, slot, g, N, lane, x, gcol, es, store_ok);
+        if (AXIS == 0) {
+            // the slot now holds the results: make them visible to the TMA store
+            fence_proxy_async();
             __syncwarp();
-            if (!bline) bulk_g2s(tile + lane * S, gl, P * 4, bar);
-            if (!mbar_wait(bar, parity, a.err, 1)) return;
-            parity ^= 1;
-        }
-        // Setboundary (include/LODkernel.cuh:112-136) and meshupdatekernel (:24-31), one line at
-        // a time across the warp; the uptake map is read only on lines that hold cells.
-        for (int r = 0; r < 32; ++r) {
-            const long long ln = tt * 32 + r;
-            if (ln >= nlines) break;
-            const int yr = (int)(ln % N), zr = (int)(ln / N);
-            const bool blr = yr < 2 || yr >= N - 2 || zr < 2 || zr >= N - 2;
-            const bool fl = sd.line_flag[ln] != 0;
-            const float* rl = sd.rate + ln * P;
-            float* row = tile + r * S;
-            for (int i = lane; i < N; i += 32) {
-                float v = (blr || i < 2 || i >= N - 2) ? sd.b : row[i];
-                if (fl) v = __fdiv_rn(v, __fmaf_rn(-rl[i], a.dt, 1.f));
-                row[i] = v;
+            if (lane == 0) {
+                box_store<AXIS>(a, d, g, slot);
+                bulk_commit();
+                if (has_next && g + 1 <= B - 1) {
+                    // the store of group g+1 has read its slot: refill it with the next tile
+                    bulk_wait_read<1>();
+                    box_load<AXIS>(a, dn, B - 2 - g, slot_of(g + 1, Q), bars + (B - 2 - g));
+                }
             }
+            __syncwarp();
+        } else {
+            // every lane has read the slot: refill it with the next tile's group
+            __syncwarp();
+            if (lane == 0 && has_next) box_load<AXIS>(a, dn, B - 1 - g, slot, bars + (B - 1 - g));
         }
-        __syncwarp();
-        if (valid) thomas_row(tile + lane * S, E, F, sd.side, sd.b, N);
-        fence_proxy_async();
-        __syncwarp();
-        if (valid) {
-            bulk_s2g(gl, tile + lane * S, P * 4);
-            bulk_commit();
-            bulk_wait_read0();
+    }
+    if (AXIS == 0) {
+        if (lane == 0) {
+            bulk_wait_read<0>();
+            if (has_next) box_load<AXIS>(a, dn, B - 1, slot_of(0, Q), bars + (B - 1));
         }
         __syncwarp();
     }
+    return true;
 }
 
-// y sweep (axis 1: lines (x, z), element stride P) or z sweep (axis 2: lines (x, y) flattened to
-// x + y*P, element stride P*N).  A warp owns 32 neighbouring lines: row j of its tile is the
-// 128-byte run of element j of those lines.
-__global__ void __launch_bounds__(512) k_sweep_strided(LodArgs a, int axis) {
-    extern __shared__ __align__(128) unsigned char sm[];
+template <int AXIS>
+__global__ void __launch_bounds__(256, 1) k_sweep(const __grid_constant__ LodArgs a) {
+    extern __shared__ __align__(1024) unsigned char sm[];
     const Geom g = a.g;
     const int N = g.N, P = g.P;
+    const int Na = (N + 31) & ~31;  // per substrate: E[Na] in shared memory
+    const int B = (N + 31) >> 5;
     const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float* sEF = reinterpret_cast<float*>(sm);
-    const int efb = align128(a.nsub * 2 * N * 4);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + efb) + warp * kChunks;
-    float* tile = reinterpret_cast<float*>(sm + efb + align128(warps * kChunks * 8)) + (size_t)warp * N * 32;
-    load_ef(sEF, a);
-    if (lane < kChunks) mbar_init(bar + lane, 1);
+    // 1024-byte aligned slots first (the x boxes use the 128-byte swizzle), then tables, barriers
+    const uint32_t base = smem_u32(sm);
+    unsigned char* sm1 = sm + ((1024 - (base & 1023)) & 1023);
+    float* buf = reinterpret_cast<float*>(sm1) + (size_t)warp * B * kSlotFloats;
+    float* sEFR = reinterpret_cast<float*>(sm1 + (size_t)warps * B * kSlotFloats * 4);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sm1 + (size_t)warps * B * kSlotFloats * 4 +
+                                                 align128(a.nsub * Na * 4)) + warp * 32;
+    for (int i = threadIdx.x; i < a.nsub * Na; i += blockDim.x) {
+        const int s = i / Na, j = i - s * Na;
+        // E of the elements the reference's recurrences update; 0 elsewhere (identity)
+        sEFR[i] = (j >= 1 && j <= N - 2) ? a.sub[s].EFR[j] : 0.f;
+    }
+    if (lane < B) mbar_init(bars + lane, 1u);
     fence_mbar_init();
     __syncthreads();
 
-    const int ntx = (P + 31) / 32;
-    const long long per_sub = axis == 1 ? (long long)ntx * N : (g.PN + 31) / 32;
+    long long per_sub;
+    if (AXIS == 0) per_sub = ((long long)N * N + 31) / 32;
+    else if (AXIS == 1) per_sub = (long long)((P + 31) / 32) * N;
+    else per_sub = (g.PN + 31) / 32;
     const long long total = per_sub * a.nsub;
-    const int R = (N - 2 + kChunks - 1) / kChunks;  // rows per chunk over rows 1..N-2
-    uint32_t parity = 0;
-    for (long long t = (long long)blockIdx.x * warps + warp; t < total; t += (long long)gridDim.x * warps) {
-        const int s = (int)(t / per_sub);
-        const long long tt = t - s * per_sub;
-        const SubDev sd = a.sub[s];
-        const float* E = sEF + s * 2 * N;
-        const float* F = E + N;
-        float* base;
-        long long rs;
-        int width;
-        bool valid;
-        if (axis == 1) {
-            const int z = (int)(tt / ntx), x0 = (int)(tt - (long long)z * ntx) * 32;
-            base = sd.p + x0 + (long long)z * g.PN;
-            rs = P;
-            width = min(32, P - x0);
-            valid = x0 + lane < N;
-        } else {
-            const long long L0 = tt * 32;
-            base = sd.p + L0;
-            rs = g.PN;
-            width = (int)min(32LL, g.PN - L0);
-            const long long L = L0 + lane;
-            valid = L < g.PN && (int)(L % P) < N;
-        }
-        if (lane == 0) {
-            for (int c = 0; c < kChunks; ++c) {
-                const int lo = 1 + c * R, hi = min(N - 1, lo + R);
-                if (hi > lo) mbar_arrive_expect(bar + c, (uint32_t)(hi - lo) * width * 4);
+    const long long step = (long long)gridDim.x * warps;
+    long long t = (long long)blockIdx.x * warps + warp;
+    if (t >= total) return;
+
+    TileDesc d = tile_desc<AXIS>(a, t, per_sub);
+    if (lane == 0)
+        for (int gi = 0; gi < B; ++gi) box_load<AXIS>(a, d, gi, buf + (size_t)gi * kSlotFloats, bars + gi);
+    __syncwarp();
+    uint32_t ph = 0;
+    int q = 0;
+    for (;;) {
+        const long long tn = t + step;
+        const bool has_next = tn < total;
+        const TileDesc dn = has_next ? tile_desc<AXIS>(a, tn, per_sub) : d;
+        const bool ok = q == 0 ? run_tile<AXIS, 0>(a, d, dn, has_next, buf, bars, ph, sEFR, Na)
+                               : run_tile<AXIS, 1>(a, d, dn, has_next, buf, bars, ph, sEFR, Na);
+        if (!ok || !has_next) break;
+        t = tn;
+        d = dn;
+        q ^= 1;
+    }
+    // no bulk store may outlive the CTA's shared memory
+    if (lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    __syncwarp();
+}
+
+// Markstein division against IEEE division on random operands in the sweeps' range.
+__global__ void k_div_check(long long n, unsigned long long seed, unsigned long long* bad) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint4 r = philox4x32_10(make_uint4((uint32_t)i, (uint32_t)(i >> 32), 7u, 0u),
+                                  make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+    // dividend: any sign, magnitudes 2^-20 .. 2^20; divisor: 1 .. 64 (F_i of the sweeps)
+    const float a = __uint_as_float((r.x & 0x80000000u) | ((107u + (r.y % 41u)) << 23) | (r.z & 0x7fffffu));
+    const float f = __uint_as_float((127u + (r.w % 6u)) << 23 | (r.x & 0x7fffffu));
+    const float y = __frcp_rn(f);
+    if (__float_as_uint(div_rn(a, f, y)) != __float_as_uint(__fdiv_rn(a, f))) atomicAdd(bad, 1ull);
+}
+
+// Setboundary + meshupdatekernel on the x-lines that hold uptake (the lines PreLOD listed), in
+// place, one line per warp: p = (boundary ? b : p) / fma(-rate, dt, 1).  Runs before the x sweep,
+// which then leaves these lines as they are (apart from elements 0 and N-1).
+struct SrcArgs {
+    float* p[kMaxSub];
+    const float* rate[kMaxSub];
+    const int* list[kMaxSub];
+    const int* count[kMaxSub];
+    float b[kMaxSub];
+    int nsub;
+    Geom g;
+    float dt;
+};
+
+__global__ void k_source_lines(SrcArgs a) {
+    const int N = a.g.N, P = a.g.P;
+    const int lane = threadIdx.x & 31;
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (int s = 0; s < a.nsub; ++s) {
+        const int cnt = *a.count[s];
+        for (long long li = gw; li < cnt; li += nw) {
+            const int line = a.list[s][li];
+            const int y = line % N, z = line / N;
+            const bool bl = y < 2 || y >= N - 2 || z < 2 || z >= N - 2;
+            float* pl = a.p[s] + (long long)line * P;
+            const float* rl = a.rate[s] + (long long)line * P;
+            for (int j = lane; j < N; j += 32) {
+                const float v = (bl || j < 2 || j > N - 3) ? a.b[s] : pl[j];
+                pl[j] = __fdiv_rn(v, __fmaf_rn(-rl[j], a.dt, 1.f));
             }
         }
-        __syncwarp();
-        for (int j = 1 + lane; j <= N - 2; j += 32)
-            bulk_g2s(tile + j * 32, base + j * rs, width * 4, bar + (j - 1) / R);
-        // forward elimination, chunk by chunk as the rows land
-        float Y = sd.b;
-        for (int c = 0; c < kChunks; ++c) {
-            const int lo = 1 + c * R, hi = min(N - 1, lo + R);
-            if (hi <= lo) break;
-            if (!mbar_wait(bar + c, (parity >> c) & 1u, a.err, 2)) return;
-            parity ^= 1u << c;
-            for (int j = lo; j < hi; ++j) {
-                Y = __fmaf_rn(-E[j], Y, tile[j * 32 + lane]);
-                tile[j * 32 + lane] = Y;
-            }
-        }
-        // back substitution, written straight to global memory (a 128-byte row per element)
-        float x = sd.b;
-        float* gp = base + lane;
-        if (valid) gp[(long long)(N - 1) * rs] = x;
-        for (int j = N - 2; j >= 1; --j) {
-            x = __fdiv_rn(__fmaf_rn(-sd.side, x, tile[j * 32 + lane]), F[j]);
-            if (valid) gp[(long long)j * rs] = x;
-        }
-        if (valid) gp[0] = sd.b;
-        fence_proxy_async();
-        __syncwarp();
     }
 }
 
@@ -387,52 +667,79 @@ gell_status prelod(gell_ctx* c, int sub) {
 
 gell_status lod_solver(gell_ctx* c, int sub, int substeps) {
     if (c->subs.empty() || substeps == 0) return GELL_OK;
-    LodArgs a{};
+    LodArgs ax{}, ay{}, az{};
     int s0 = sub < 0 ? 0 : sub, s1 = sub < 0 ? (int)c->subs.size() : sub + 1;
-    for (int s = s0; s < s1; ++s) {
+    int ns = 0;
+    for (int s = s0; s < s1; ++s, ++ns) {
         const Substrate& S = c->subs[s];
-        a.sub[a.nsub++] = SubDev{S.p, S.rate, S.line_flag, S.EF, S.s.boundary, S.side};
+        const SubDev sd{S.p, S.rate, S.line_flag, S.EF, S.FRS, S.s.boundary, S.side};
+        ax.sub[ns] = ay.sub[ns] = az.sub[ns] = sd;
+        ax.tm[ns] = S.tmap[0];
+        ay.tm[ns] = S.tmap[1];
+        az.tm[ns] = S.tmap[2];
     }
-    a.g = c->g;
-    a.dt = c->P.diffusion_dt;
-    a.err = c->dev_err;
+    for (LodArgs* a : {&ax, &ay, &az}) {
+        a->nsub = ns;
+        a->g = c->g;
+        a->dt = c->P.diffusion_dt;
+        a->err = c->dev_err;
+    }
     const int N = c->g.N;
-    const int efb = align128(a.nsub * 2 * N * 4);
+    const int B = (N + 31) / 32;
+    const int Na = (N + 31) & ~31;
     const int smem_cap = 227 * 1024;
-    // x: [32][S] per warp
-    const int xtile = 32 * xrow_stride(c->g.P) * 4;
-    int wx = (smem_cap - efb - 128) / xtile;
-    wx = wx > 16 ? 16 : wx;
-    // y/z: [N][32] per warp
-    const int stile = N * 32 * 4;
-    int ws = (smem_cap - efb - 128 * 2) / stile;
-    ws = ws > 16 ? 16 : ws;
-    if (wx < 1 || ws < 1) return fail(c, GELL_ERR_UNSUPPORTED, "grid edge too large for the shared-memory line tiles");
-    const int smx = efb + align128(wx * 8) + wx * xtile;
-    const int sms = efb + align128(ws * kChunks * 8) + ws * stile;
-    static int configured = 0;
+    const int fixed = 1024 + align128(ns * Na * 4) + 16 * 32 * 8;
+    int w = (smem_cap - fixed) / (B * kSlotFloats * 4);
+    w = w > 8 ? 8 : w;
+    if (w < 1) return fail(c, GELL_ERR_UNSUPPORTED, "grid edge too large for the shared-memory line tiles");
+    const int smem = 1024 + w * B * kSlotFloats * 4 + align128(ns * Na * 4) + align128(w * 32 * 8);
+    static bool configured = false;
     if (!configured) {
-        GELL_CUDA(c, cudaFuncSetAttribute(k_sweep_x, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
-        GELL_CUDA(c, cudaFuncSetAttribute(k_sweep_strided, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
-        configured = 1;
+        GELL_CUDA(c, cudaFuncSetAttribute(k_sweep<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
+        GELL_CUDA(c, cudaFuncSetAttribute(k_sweep<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
+        GELL_CUDA(c, cudaFuncSetAttribute(k_sweep<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
+        configured = true;
     }
-    const long long nlines = (long long)N * N;
-    const long long xt = (nlines + 31) / 32 * a.nsub;
-    const long long yt = (long long)((c->g.P + 31) / 32) * N * a.nsub;
-    const long long zt = (c->g.PN + 31) / 32 * a.nsub;
-    auto grid = [&](long long tiles, int w, int smem) {
-        int per_sm = smem_cap / (smem + 1024);
-        if (per_sm < 1) per_sm = 1;
+    const long long xt = ((long long)N * N + 31) / 32 * ns;
+    const long long yt = (long long)((c->g.P + 31) / 32) * N * ns;
+    const long long zt = (c->g.PN + 31) / 32 * ns;
+    auto grid = [&](long long tiles) {
         long long want = (tiles + w - 1) / w;
-        long long cap = (long long)num_sms() * per_sm;
+        long long cap = num_sms();
         return (int)(want < cap ? want : cap);
     };
-    const int gx = grid(xt, wx, smx), gy = grid(yt, ws, sms), gz = grid(zt, ws, sms);
-    for (int k = 0; k < substeps; ++k) {
-        GELL_KERNEL(c, "k_sweep_x", k_sweep_x<<<gx, wx * 32, smx, c->stream>>>(a));
-        GELL_KERNEL(c, "k_sweep_strided(y)", k_sweep_strided<<<gy, ws * 32, sms, c->stream>>>(a, 1));
-        GELL_KERNEL(c, "k_sweep_strided(z)", k_sweep_strided<<<gz, ws * 32, sms, c->stream>>>(a, 2));
+    const int gx = grid(xt), gy = grid(yt), gz = grid(zt);
+    SrcArgs sa{};
+    for (int s = s0; s < s1; ++s) {
+        const Substrate& S = c->subs[s];
+        sa.p[sa.nsub] = S.p;
+        sa.rate[sa.nsub] = S.rate;
+        sa.list[sa.nsub] = S.line_list;
+        sa.count[sa.nsub] = S.line_count;
+        sa.b[sa.nsub] = S.s.boundary;
+        sa.nsub++;
     }
+    sa.g = c->g;
+    sa.dt = c->P.diffusion_dt;
+    for (int k = 0; k < substeps; ++k) {
+        GELL_KERNEL(c, "k_source_lines", k_source_lines<<<num_sms() * 2, 256, 0, c->stream>>>(sa));
+        GELL_KERNEL(c, "k_sweep_x", k_sweep<0><<<gx, w * 32, smem, c->stream>>>(ax));
+        GELL_KERNEL(c, "k_sweep_y", k_sweep<1><<<gy, w * 32, smem, c->stream>>>(ay));
+        GELL_KERNEL(c, "k_sweep_z", k_sweep<2><<<gz, w * 32, smem, c->stream>>>(az));
+    }
+    return GELL_OK;
+}
+
+gell_status selftest_division(gell_ctx* c, long long n, unsigned long long seed, long long* mismatches) {
+    unsigned long long* d = nullptr;
+    GELL_CUDA(c, cudaMallocAsync((void**)&d, 8, c->stream));
+    GELL_CUDA(c, cudaMemsetAsync(d, 0, 8, c->stream));
+    GELL_KERNEL(c, "k_div_check", k_div_check<<<(int)((n + 255) / 256), 256, 0, c->stream>>>(n, seed, d));
+    unsigned long long h = 0;
+    GELL_CUDA(c, cudaMemcpyAsync(&h, d, 8, cudaMemcpyDeviceToHost, c->stream));
+    GELL_CUDA(c, cudaFreeAsync(d, c->stream));
+    GELL_CUDA(c, cudaStreamSynchronize(c->stream));
+    *mismatches = (long long)h;
     return GELL_OK;
 }
 

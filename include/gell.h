@@ -219,6 +219,11 @@ typedef struct gell_profile_record {
 gell_status gell_profile_enable(gell_ctx* ctx, int on);
 gell_status gell_profile_read(gell_ctx* ctx, gell_profile_record* out, int max_records, int* count,
                               int reset);
+/* Self-test of the division the LOD back substitution uses (a Markstein division with a
+ * precomputed reciprocal) against IEEE division, on `samples` random operands in the sweeps'
+ * range; *mismatches = number of quotients that differ in any bit.  Synchronises. */
+gell_status gell_selftest_division(gell_ctx* ctx, int64_t samples, uint64_t seed, int64_t* mismatches);
+
 /* Number of kernels this context has launched (always counted). */
 gell_status gell_launch_count(gell_ctx* ctx, int64_t* count);
 

@@ -164,3 +164,11 @@ def test_lod_full_size_two_substrates_vs_oracle():
             start = field if sub == 0 else field / 38.0
             exp = ol.lod_substeps(start, rate, E, F, N, 0.01, s.boundary, 2)
             assert bits_equal(sim.field(sub), exp), f"substrate {sub}"
+
+
+def test_markstein_division_matches_ieee():
+    """The back substitution divides with a precomputed reciprocal and two residual corrections;
+    it must equal IEEE round-to-nearest division bit for bit."""
+    with make_sim(16, 10.0, cap=16) as sim:
+        assert sim.selftest_division(1 << 26, seed=11) == 0
+        assert sim.selftest_division(1 << 26, seed=12) == 0
