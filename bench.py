@@ -41,10 +41,12 @@ N, LENGTH, NCELLS, SUBSTEPS, CAP = 400, 10.0, 1_000_000, 10, 2_000_000
 NSUB = 2
 WORKLOAD = ("plain method, large: 400^3 voxels at 10 um, oxygen + drug (FP32), 10^6 cells, "
             "1 mechanics step = FM_update + PreLOD + 10 LOD substeps")
-# algorithmic bytes per voxel-update of each LOD kernel: source + x sweep reads p and the uptake
-# rate and writes p (12 B); the y and z sweeps read and write p (8 B each)
-ALGO_BYTES = {"k_sweep_x": 12.0, "k_sweep_y": 8.0, "k_sweep_z": 8.0}
+# algorithmic bytes per voxel-update of each sweep: read p once and write it once (8 B).  The
+# uptake source (read rate) runs before the x sweep in k_source_lines, on the x-lines that hold
+# cells only, so the x sweep itself moves no rate bytes.
+ALGO_BYTES = {"k_sweep_x": 8.0, "k_sweep_y": 8.0, "k_sweep_z": 8.0}
 FALLBACK_HBM_GBS = 6650.0
+PROFILE_SUMMARY = "k_sweep_400cube_2sub.md"
 
 
 def config(extra=None):
@@ -69,6 +71,19 @@ def hbm_peak():
             return float(json.load(f)["hbm_gbs"]), "measured"
     except Exception:
         return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic(kernel):
+    """DRAM bytes (read + write) of one launch of `kernel` at this workload, from the committed ncu
+    summary (lines `traffic <kernel>: <bytes>`), or None when no capture is recorded."""
+    path = os.path.join(ROOT, "profiles", PROFILE_SUMMARY)
+    try:
+        for line in open(path):
+            if line.startswith(f"traffic {kernel}:"):
+                return int(line.split(":", 1)[1].split()[0]), f"profiles/{PROFILE_SUMMARY}"
+    except OSError:
+        pass
+    return None, None
 
 
 # ---------------------------------------------------------------------------- clocks
@@ -129,6 +144,17 @@ class ClockSampler:
 
 # ---------------------------------------------------------------------------- GPU arm
 
+def reduce_over_ranks(times, cells, device):
+    """Replicas: device times take the max over ranks, processed cells the sum."""
+    import torch
+    import torch.distributed as td
+    tt = torch.tensor(np.asarray(times, np.float64), device=device)
+    td.all_reduce(tt, op=td.ReduceOp.MAX)
+    cc = torch.tensor(np.asarray(cells, np.float64), device=device)
+    td.all_reduce(cc, op=td.ReduceOp.SUM)
+    return tt.cpu().numpy(), cc.cpu().numpy()
+
+
 def run_gell(args, rank, world, local_rank):
     import torch
     import gell_b200 as gb
@@ -164,8 +190,6 @@ def run_gell(args, rank, world, local_rank):
 
     K = args.steps
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(K)]
-    sim.profile(True)
-    sim.profile_read(reset=True)
     launches0 = sim.launch_count()
     if dist:
         td.barrier()
@@ -182,9 +206,18 @@ def run_gell(args, rank, world, local_rank):
     if dist:
         td.barrier()
     launches = sim.launch_count() - launches0
+    sampler.stop()
+
+    # per-kernel device times: a separate pass with an event pair around every launch, on the
+    # stream the kernels run on, so the timed region above carries no profiling events
+    kp = max(1, min(K, 10))
+    sim.profile(True)
+    sim.profile_read(reset=True)
+    for _ in range(kp):
+        step()
+    sim.sync()
     prof = sim.profile_read(reset=True)
     sim.profile(False)
-    sampler.stop()
 
     t_fm = sum(ev[k][0].elapsed_time(ev[k][1]) for k in range(K))
     t_pre = sum(ev[k][1].elapsed_time(ev[k][2]) for k in range(K))
@@ -213,12 +246,7 @@ def run_gell(args, rank, world, local_rank):
     times = np.array([t_all, t_fm + t_pre, t_lod, t_e2e], np.float64)
     cells_all = np.array([alive * K, alive * ke], np.float64)
     if dist:
-        tt = torch.tensor(times, device="cuda")
-        td.all_reduce(tt, op=td.ReduceOp.MAX)
-        times = tt.cpu().numpy()
-        cc = torch.tensor(cells_all, device="cuda")
-        td.all_reduce(cc, op=td.ReduceOp.SUM)
-        cells_all = cc.cpu().numpy()
+        times, cells_all = reduce_over_ranks(times, cells_all, "cuda")
     t_all, t_mech, t_lod, t_e2e = times
     value = cells_all[0] / (t_all / 1e3)
     mech_rate = cells_all[0] / (t_mech / 1e3)
@@ -231,8 +259,10 @@ def run_gell(args, rank, world, local_rank):
     avg_ms = ms / nl
     peak, peak_kind = hbm_peak()
     algo = ALGO_BYTES.get(name)
+    traffic, traffic_src = ncu_traffic(name)
     roof = {"kernel": name, "bound": "hbm", "launches": nl, "avg_ms": avg_ms, "peak": peak,
-            "peak_source": f"{peak_kind} hbm_gbs", "unit": "GB/s", "traffic": None}
+            "peak_source": f"{peak_kind} hbm_gbs", "unit": "GB/s", "traffic": traffic,
+            "traffic_source": traffic_src}
     if algo is not None:
         per_launch = algo * N ** 3 * NSUB
         roof.update(achieved=per_launch / (avg_ms / 1e3) / 1e9, bytes_per_launch=per_launch,

@@ -2,9 +2,10 @@
 //
 // One substep of the reference (Mesh_struct::LODsolver) is Setboundary, meshupdatekernel and the
 // three Thomas sweeps LODkernel_x/y/z, each a launch of one thread per line.  Here a substep is
-// three launches of one kernel template, all substrates in each:
-//   k_sweep<0>  boundary layers + implicit uptake source + x sweep (x-lines are contiguous)
-//   k_sweep<1>  y sweep (element stride P)      k_sweep<2>  z sweep (element stride P*N)
+// four launches, all substrates in each:
+//   k_source_lines  boundary layers + implicit uptake source on the x-lines that hold cells
+//   k_sweep<0>      boundary layers of the other lines + x sweep (x-lines are contiguous)
+//   k_sweep<1>      y sweep (element stride P)      k_sweep<2>  z sweep (element stride P*N)
 //
 // Streaming line tiles.  A warp owns a tile of 32 lines (one per lane) and walks its lane's line
 // out of shared memory.  The line is cut into B = ceil(N/32) groups of 32 elements; each group of
@@ -569,9 +570,22 @@ __global__ void k_source_lines(SrcArgs a) {
             const bool bl = y < 2 || y >= N - 2 || z < 2 || z >= N - 2;
             float* pl = a.p[s] + (long long)line * P;
             const float* rl = a.rate[s] + (long long)line * P;
-            for (int j = lane; j < N; j += 32) {
-                const float v = (bl || j < 2 || j > N - 3) ? a.b[s] : pl[j];
-                pl[j] = __fdiv_rn(v, __fmaf_rn(-rl[j], a.dt, 1.f));
+            for (int j0 = 0; j0 < N; j0 += 32 * 8) {
+                float pv[8], rv[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const int j = j0 + 32 * k + lane;
+                    pv[k] = j < N ? pl[j] : 0.f;
+                    rv[k] = j < N ? rl[j] : 0.f;
+                }
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const int j = j0 + 32 * k + lane;
+                    if (j < N) {
+                        const float v = (bl || j < 2 || j > N - 3) ? a.b[s] : pv[k];
+                        pl[j] = __fdiv_rn(v, __fmaf_rn(-rv[k], a.dt, 1.f));
+                    }
+                }
             }
         }
     }
@@ -722,7 +736,7 @@ gell_status lod_solver(gell_ctx* c, int sub, int substeps) {
     sa.g = c->g;
     sa.dt = c->P.diffusion_dt;
     for (int k = 0; k < substeps; ++k) {
-        GELL_KERNEL(c, "k_source_lines", k_source_lines<<<num_sms() * 2, 256, 0, c->stream>>>(sa));
+        GELL_KERNEL(c, "k_source_lines", k_source_lines<<<num_sms() * 8, 256, 0, c->stream>>>(sa));
         GELL_KERNEL(c, "k_sweep_x", k_sweep<0><<<gx, w * 32, smem, c->stream>>>(ax));
         GELL_KERNEL(c, "k_sweep_y", k_sweep<1><<<gy, w * 32, smem, c->stream>>>(ay));
         GELL_KERNEL(c, "k_sweep_z", k_sweep<2><<<gz, w * 32, smem, c->stream>>>(az));

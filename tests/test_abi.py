@@ -112,3 +112,51 @@ def test_null_context_calls_are_rejected():
                      ("gell_cell_birth", [None]), ("gell_cell_death", [None]), ("gell_sync", []),
                      ("gell_destroy", [])):
         assert getattr(lib, fn)(None, *args) == -1, fn
+
+
+COMPAT_MAIN = r"""
+#include <cstdio>
+#include "gell_compat.hpp"
+int main() {
+    try {
+        gell::Context ctx(gell::reference_params());
+        gell::MechanicsMesh_struct mec(ctx);
+        gell::Mesh_struct o2(ctx, 38.f, 1e5f, 0.1f);
+        mec.FM_update();
+        o2.PreLOD();
+        o2.LODsolver();
+        int n = gell::CellBirth_kernel(ctx);
+        n = gell::CellDeath_kernel(ctx);
+        std::printf("ran %d\n", n);
+        return 0;
+    } catch (const gell::Error& e) {
+        std::printf("status %d\n", (int)e.status);
+        return 3;
+    }
+}
+"""
+
+
+def test_compat_header_builds_a_reference_shaped_loop(tmp_path):
+    """include/gell_compat.hpp compiles with plain g++ against the C ABI; without a GPU the first
+    call throws gell::Error carrying GELL_ERR_NO_DEVICE."""
+    import shutil
+    import subprocess
+    gb = pytest.importorskip("gell_b200")
+    libpath = gb.load_library()._name
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("g++ missing")
+    src = tmp_path / "main.cpp"
+    src.write_text(COMPAT_MAIN)
+    exe = tmp_path / "main"
+    cuda_lib = "/usr/local/cuda/lib64"
+    r = subprocess.run([gxx, "-std=c++17", "-O1", f"-I{os.path.join(ROOT, 'include')}", str(src),
+                        libpath, f"-L{cuda_lib}", "-lcudart", f"-Wl,-rpath,{os.path.dirname(libpath)}",
+                        f"-Wl,-rpath,{cuda_lib}", "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present: the no-device path is not reachable")
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 3 and r.stdout.strip() == "status -4", (r.returncode, r.stdout, r.stderr)
