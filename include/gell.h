@@ -224,6 +224,25 @@ gell_status gell_profile_read(gell_ctx* ctx, gell_profile_record* out, int max_r
  * range; *mismatches = number of quotients that differ in any bit.  Synchronises. */
 gell_status gell_selftest_division(gell_ctx* ctx, int64_t samples, uint64_t seed, int64_t* mismatches);
 
+/* Largest key count gell_sort_keys_noalloc accepts. */
+#define GELL_NOALLOC_MAX_KEYS (1 << 20)
+
+/* Stable sort of n int32 Morton keys (-1 = outside the grid, ordered first) into sorted_keys,
+ * with perm[i] = input position of sorted position i: the sort FM_update performs, for callers
+ * that cannot allocate device memory.  No counterpart in the reference (its thrust::sort_by_key
+ * allocates temporary storage on every call, include/FMkernel.cuh:190).  Some callers cannot call
+ * cudaMalloc when they need the sort: code that runs while a CUDA stream is being captured, hosts
+ * that must keep to a memory budget reserved up front, C callers that only own their buffers.  So
+ * this call allocates nothing: keys, sorted_keys and perm are the caller's device buffers, and the
+ * scratch lives in one fixed device array inside the library (about 8.3 MB on every GPU that
+ * loads it, kept until the process exits).  key_bits = bits of the largest key + 1 (e.g. 28 on a
+ * 400^3 grid).  n above GELL_NOALLOC_MAX_KEYS returns GELL_ERR_CAPACITY.  The first call on a
+ * device looks up that device's scratch address and should come before any stream capture; all
+ * calls share the scratch, so calls that overlap on the GPU race.  Work is queued on `stream`
+ * (a cudaStream_t; NULL = the default stream) and not synchronised. */
+gell_status gell_sort_keys_noalloc(const int32_t* keys, int32_t* sorted_keys, int32_t* perm, int n,
+                                   int key_bits, void* stream);
+
 /* Number of kernels this context has launched (always counted). */
 gell_status gell_launch_count(gell_ctx* ctx, int64_t* count);
 
