@@ -131,13 +131,14 @@ def load_library() -> ctypes.CDLL:
     L.gell_profile_enable.argtypes = [P, ctypes.c_int]
     L.gell_profile_read.argtypes = [P, P, ctypes.c_int, P, ctypes.c_int]
     L.gell_launch_count.argtypes = [P, P]
+    L.gell_set_option.argtypes = [P, ctypes.c_int, ctypes.c_int64]
     L.gell_selftest_division.argtypes = [P, ctypes.c_int64, ctypes.c_uint64, P]
     for name in ("gell_create", "gell_destroy", "gell_set_stream", "gell_substrate_add",
                  "gell_cells_import", "gell_cells_export", "gell_cell_count", "gell_field_import",
                  "gell_field_export", "gell_fm_update", "gell_prelod", "gell_lod_solver",
                  "gell_cell_birth", "gell_cell_death", "gell_mechanics_step", "gell_sync",
                  "gell_debug_dump", "gell_profile_enable", "gell_profile_read", "gell_launch_count",
-                 "gell_selftest_division"):
+                 "gell_selftest_division", "gell_set_option"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
@@ -296,6 +297,10 @@ class Simulation:
         self._check(self.lib.gell_selftest_division(self.h, samples, seed, ctypes.byref(m)),
                     "gell_selftest_division")
         return m.value
+
+    def set_exact_chain(self, on: bool = True) -> None:
+        """Run every LOD back-substitution group on the exact division chain (same results)."""
+        self._check(self.lib.gell_set_option(self.h, 1, int(bool(on))), "gell_set_option")
 
     def launch_count(self) -> int:
         v = ctypes.c_int64()

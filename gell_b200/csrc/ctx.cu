@@ -325,6 +325,12 @@ static void mesh_init(int N, float len, float D, float decay, float dt, std::vec
 
 // RN(1/f): the float nearest to 1/f.  The product of two floats is exact in double, so
 // |1 - y*f| ranks the candidates exactly; 1/f of a float is never halfway between two floats.
+static uint32_t bits_of(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    return u;
+}
+
 static float recip_rn(float f) {
     const float y0 = (float)(1.0 / (double)f);
     float best = y0;
@@ -414,8 +420,17 @@ gell_status gell_substrate_add(gell_ctx* c, const gell_substrate* s, int* index_
         std::vector<float4> frs((size_t)Na);
         for (int j = 0; j < Na; ++j) {
             const bool in = j >= 1 && j <= c->g.N - 2;
-            frs[j] = in ? make_float4(sub.F[j], efr[2 * c->g.N + j], sub.side, 0.f) : make_float4(1.f, 1.f, 0.f, 0.f);
+            const float rj = efr[2 * c->g.N + j];
+            frs[j] = in ? make_float4(sub.F[j], rj, sub.side, sub.side * rj) : make_float4(1.f, 1.f, 0.f, 0.f);
         }
+        const int N = c->g.N;
+        const uint32_t eb = bits_of(sub.E[N - 2]), fb2 = bits_of(sub.F[N - 2]);
+        for (int g = 0; 32 * g < N; ++g) {
+            bool uni = 32 * g >= 1 && 32 * g + 31 <= N - 2;
+            for (int j = 32 * g; uni && j < 32 * g + 32; ++j) uni = bits_of(sub.E[j]) == eb && bits_of(sub.F[j]) == fb2;
+            if (uni) sub.uniform_groups |= 1u << g;
+        }
+        sub.conv_R = recip_rn(sub.F[N - 2]);
         GELL_CUDA(c, cudaMalloc(&sub.FRS, frs.size() * sizeof(float4)));
         GELL_CUDA(c, cudaMemcpy(sub.FRS, frs.data(), frs.size() * sizeof(float4), cudaMemcpyHostToDevice));
     }
@@ -545,6 +560,14 @@ gell_status gell_selftest_division(gell_ctx* c, int64_t samples, uint64_t seed, 
     gell_status st = selftest_division(c, samples, seed, &m);
     *mismatches = m;
     return st;
+}
+
+gell_status gell_set_option(gell_ctx* c, int option, int64_t value) {
+    if (!c) return GELL_ERR_INVALID_ARG;
+    switch (option) {
+        case GELL_OPT_EXACT_CHAIN: c->exact_chain = value != 0; return GELL_OK;
+        default: return fail(c, GELL_ERR_INVALID_ARG, "unknown option");
+    }
 }
 
 gell_status gell_launch_count(gell_ctx* c, int64_t* count) {

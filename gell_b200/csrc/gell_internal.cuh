@@ -54,13 +54,18 @@ struct Substrate {
     float* p = nullptr;     // field, pitched
     float* rate = nullptr;  // uptake map, pitched; nonzero only on flagged lines
     float* EF = nullptr;    // device: E[N], F[N], RN(1/F)[N]
-    float4* FRS = nullptr;  // device: (F, RN(1/F), s, 0) per element of 32*ceil(N/32), boundary
+    float4* FRS = nullptr;  // device: (F, RN(1/F), s, s*RN(1/F)) per element of 32*ceil(N/32), boundary
                             // elements (0 and >= N-1) as identities (1, 1, 0, 0)
     uint32_t* line_flag = nullptr;  // N*N: x-line (y + z*N) holds uptake
     int* line_list = nullptr;       // flagged lines
     int* line_count = nullptr;      // device: number of flagged lines
     std::vector<float> E, F;
     float side = 0.f;       // E[1]*F[0], the sweeps' off-diagonal (thomas_side)
+    // Groups of 32 elements (bit g = elements 32g..32g+31) that lie inside 1..N-2 and whose E and
+    // F equal E[N-2], F[N-2] bit for bit: the LU factors of the constant-coefficient line converge
+    // within a few dozen elements, so all groups but the first and the last usually qualify.
+    uint32_t uniform_groups = 0;
+    float conv_R = 0.f;     // RN(1/F[N-2]), the reciprocal of the converged F
     CUtensorMap tmap[3];    // TMA maps of the field for the x, y and z sweeps (32x32 boxes)
 };
 
@@ -106,6 +111,7 @@ struct gell_ctx {
 
     std::vector<gell::Substrate> subs;
     bool rate_valid = false;
+    bool exact_chain = false;  // GELL_OPT_EXACT_CHAIN
 
     // PD
     curandState* xorwow = nullptr;

@@ -44,9 +44,13 @@ struct SubDev {
     const float* rate;
     const uint32_t* line_flag;
     const float* EFR;  // E[N], F[N], RN(1/F)[N]
-    const float4* FRS; // per element (F, RN(1/F), s, 0), boundary elements as identities
+    const float4* FRS; // per element (F, RN(1/F), s, s*RN(1/F)), boundary elements as identities
     float b;
     float side;
+    // groups whose E, F are the line's converged constants, and those constants pre-negated:
+    // -E, -s, -s*RN(1/F), -F and RN(1/F)
+    uint32_t uni;
+    float nE, nS, nSR, nF, R;
 };
 
 struct LodArgs {
@@ -56,6 +60,7 @@ struct LodArgs {
     Geom g;
     float dt;
     int* err;
+    int exact;  // every group on the exact chain (GELL_OPT_EXACT_CHAIN)
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -84,6 +89,16 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
         : "r"(smem_u32(b)), "r"(parity)
         : "memory");
     return ok != 0;
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+// Bounded wait of a single thread on an mbarrier phase; records `code` and returns false on timeout.
+__device__ __forceinline__ bool mbar_wait1(uint64_t* b, uint32_t parity, int* err, int code) {
+    for (int it = 0; it < (1 << 24); ++it)
+        if (mbar_try_wait(b, parity)) return true;
+    atomicExch(err, code);
+    return false;
 }
 // Bounded, warp-uniform wait on an mbarrier phase: every lane polls until all lanes see the phase
 // complete; after a fixed number of polls the warp gives up together, records `code` in the
@@ -144,11 +159,9 @@ struct TileDesc {
     long long line;                    // x: this lane's line (y + z*N)
 };
 
+// Substrate and TMA coordinates of tile t.
 template <int AXIS>
-__device__ __forceinline__ TileDesc tile_desc(const LodArgs& a, long long t, long long per_sub) {
-    const Geom& g = a.g;
-    const int N = g.N, P = g.P;
-    const int lane = threadIdx.x & 31;
+__device__ __forceinline__ TileDesc tile_coords(const LodArgs& a, long long t, long long per_sub) {
     TileDesc d;
     d.s = (int)(t / per_sub);
     const long long tt = t - d.s * per_sub;
@@ -156,19 +169,29 @@ __device__ __forceinline__ TileDesc tile_desc(const LodArgs& a, long long t, lon
     d.interior_lane = d.flagged_lane = false;
     d.line = 0;
     if (AXIS == 0) {
-        const long long nl = (long long)N * N;
         d.c0 = (int)(tt * 32);
-        d.line = (long long)d.c0 + lane;
-        const bool valid = d.line < nl;
-        const int y = valid ? (int)(d.line % N) : 0, z = valid ? (int)(d.line / N) : 0;
-        d.interior_lane = valid && y >= 2 && y < N - 2 && z >= 2 && z < N - 2;
-        d.flagged_lane = valid && a.sub[d.s].line_flag[d.line] != 0u;
     } else if (AXIS == 1) {
-        const int ntx = (P + 31) / 32;
+        const int ntx = (a.g.P + 31) / 32;
         d.c2 = (int)(tt / ntx);
         d.c0 = (int)(tt - (long long)d.c2 * ntx) * 32;
     } else {
         d.c0 = (int)(tt * 32);
+    }
+    return d;
+}
+
+// ... and, for x, what this lane's line is (interior, holds uptake).
+template <int AXIS>
+__device__ __forceinline__ TileDesc tile_desc(const LodArgs& a, long long t, long long per_sub) {
+    TileDesc d = tile_coords<AXIS>(a, t, per_sub);
+    if (AXIS == 0) {
+        const int N = a.g.N;
+        const long long nl = (long long)N * N;
+        d.line = (long long)d.c0 + (threadIdx.x & 31);
+        const bool valid = d.line < nl;
+        const int y = valid ? (int)(d.line % N) : 0, z = valid ? (int)(d.line / N) : 0;
+        d.interior_lane = valid && y >= 2 && y < N - 2 && z >= 2 && z < N - 2;
+        d.flagged_lane = valid && a.sub[d.s].line_flag[d.line] != 0u;
     }
     return d;
 }
@@ -231,33 +254,27 @@ __device__ __forceinline__ void store8(float* slot, int e0, int lane, const floa
     }
 }
 
-// x: Setboundary for lines without uptake, in place on group g of the tile, one line at a time
-// across the warp (lane = element): the two outer layers of every face hold b.  Lines with uptake
-// were prepared by k_source_lines (boundary and source already applied); for them only elements 0
-// and N-1 are set, to the reference's Y_0 = b and x_{N-1} = b.
-__device__ __forceinline__ void x_prepass(const SweepCtx& c, float* slot, int g, int N, uint32_t lines,
-                                          uint32_t interior, uint32_t flagged) {
-    const int lane = threadIdx.x & 31;
-    const int j = 32 * g + lane;
-    const bool outer = j < 2 || j > N - 3;
-    const bool ends = j == 0 || j >= N - 1;
-    while (lines) {
-        const int r = __ffs(lines) - 1;
-        lines &= lines - 1;
-        float* p = slot + r * 32 + (((lane >> 2) ^ (r & 7)) << 2) + (lane & 3);
-        if ((flagged >> r) & 1u) {
-            if (ends) *p = c.b;
-        } else if (!((interior >> r) & 1u) || outer) {
-            *p = c.b;
-        }
-    }
-    __syncwarp();
+// x: Setboundary on the values the forward elimination loads.  Element j of this lane's line is
+// replaced by b when j < lo or j > hi: lo = 2, hi = N-3 for interior lines without uptake (the two
+// outer layers of the y/z faces); lo = 1, hi = N-2 for lines with uptake, which k_source_lines has
+// already prepared (only the reference's Y_0 = b and x_{N-1} = b remain); lo = INT_MAX for the
+// boundary lines themselves, all of whose elements are b.  `rs` (warp-uniform) says whether any
+// lane resets an element of this group.
+struct XReset {
+    int lo, hi;
+    float b;
+};
+
+__device__ __forceinline__ void reset8(float v[8], int j0, const XReset& r) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = (j0 + k < r.lo || j0 + k > r.hi) ? r.b : v[k];
 }
 
 // Forward elimination over group g: Y_j = fma(-E_j, Y_{j-1}, p_j) for the 32 elements of the group,
 // 8 at a time with the next batch's values and E already requested.
 template <int AXIS>
-__device__ __forceinline__ void forward_group(const SweepCtx& c, float* slot, int g, int lane, float& Y) {
+__device__ __forceinline__ void forward_group(const SweepCtx& c, float* slot, int g, int lane, float& Y, bool rs,
+                                              const XReset& xr) {
     const int j0 = 32 * g;
     float v[8], w[8];
     float4 e0 = *reinterpret_cast<const float4*>(c.E + j0);
@@ -271,6 +288,7 @@ __device__ __forceinline__ void forward_group(const SweepCtx& c, float* slot, in
             n0 = *reinterpret_cast<const float4*>(c.E + j0 + 8 * b8 + 8);
             n1 = *reinterpret_cast<const float4*>(c.E + j0 + 8 * b8 + 12);
         }
+        if (AXIS == 0 && rs) reset8(v, j0 + 8 * b8, xr);
         const float ev[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
@@ -298,7 +316,7 @@ __device__ __forceinline__ float back_exact(float x, float y, float f, float rf,
 // the whole group is recomputed on the exact chain, so o[] always holds the exact values.
 template <int AXIS>
 __device__ __forceinline__ void backward_full(const SweepCtx& c, float* slot, int j0, int lane, float& x,
-                                              float o[32]) {
+                                              float o[32], int exact) {
     const float x_in = x;
     uint32_t bad = 0;
     float v[8], w[8];
@@ -314,16 +332,13 @@ __device__ __forceinline__ void backward_full(const SweepCtx& c, float* slot, in
 #pragma unroll
             for (int k = 0; k < 8; ++k) h[k] = __ldg(fb + 8 * b8 - 8 + k);
         }
-        float yr[8], sr[8];
+        float yr[8];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            yr[k] = __fmul_rn(v[k], f[k].y);
-            sr[k] = __fmul_rn(f[k].z, f[k].y);
-        }
+        for (int k = 0; k < 8; ++k) yr[k] = __fmul_rn(v[k], f[k].y);
 #pragma unroll
         for (int k = 7; k >= 0; --k) {
             const float t = __fmaf_rn(-f[k].z, x, v[k]);
-            const float a0 = __fmaf_rn(-sr[k], x, yr[k]);
+            const float a0 = __fmaf_rn(-f[k].w, x, yr[k]);
             const float r0 = __fmaf_rn(-a0, f[k].x, t);
             const float a1 = __fmaf_rn(r0, f[k].y, a0);   // carried on the chain
             const float r1 = __fmaf_rn(-a1, f[k].x, t);
@@ -340,7 +355,7 @@ __device__ __forceinline__ void backward_full(const SweepCtx& c, float* slot, in
             }
         }
     }
-    if (__any_sync(FULL, bad != 0)) {
+    if (__any_sync(FULL, bad != 0) || exact) {
         x = x_in;
 #pragma unroll
         for (int e = 31; e >= 0; --e) {
@@ -351,36 +366,93 @@ __device__ __forceinline__ void backward_full(const SweepCtx& c, float* slot, in
     }
 }
 
-// Back substitution over group g, from its top element down.  x: results go back into the slot
-// (stored by TMA afterwards); y/z: results go straight to global memory from registers, a full
-// 128-byte row per element (gcol = this lane's line at element 0, es = element stride), for the
-// elements below N.
+// The same two steps for a group whose E and F are the line's converged constants (all lanes'
+// lines share them): the factors live in registers, and independent multiply-adds are issued in
+// pairs (FFMA2), without changing any operation or its rounding.
 template <int AXIS>
-__device__ __forceinline__ void backward_group(const SweepCtx& c, float* slot, int g, int N, int lane, float& x,
-                                               float* gcol, long long es, bool store_ok) {
-    const int j0 = 32 * g;
-    float o[32];
-    backward_full<AXIS>(c, slot, j0, lane, x, o);
-    if (AXIS == 0) {
+__device__ __forceinline__ void forward_uniform(float* slot, int g, int lane, float& Y, float nE, bool rs,
+                                                const XReset& xr) {
+    float v[8], w[8];
+    load8<AXIS>(slot, 0, lane, v);
 #pragma unroll
-        for (int b8 = 0; b8 < 4; ++b8) store8<AXIS>(slot, 8 * b8, lane, o + 8 * b8);
-    } else if (store_ok) {
-        const int ne = min(32, N - j0);
-        float* gp = gcol + (long long)j0 * es;
-        if (ne == 32) {
+    for (int b8 = 0; b8 < 4; ++b8) {
+        if (b8 < 3) load8<AXIS>(slot, 8 * b8 + 8, lane, w);
+        if (AXIS == 0 && rs) reset8(v, 32 * g + 8 * b8, xr);
 #pragma unroll
-            for (int e = 0; e < 32; ++e) {
-                gp[0] = o[e];
-                gp += es;
-            }
-        } else {
+        for (int k = 0; k < 8; ++k) {
+            Y = __fmaf_rn(nE, Y, v[k]);
+            v[k] = Y;
+        }
+        store8<AXIS>(slot, 8 * b8, lane, v);
+        if (b8 < 3) {
 #pragma unroll
-            for (int e = 0; e < 32; ++e) {
-                if (e < ne) gp[0] = o[e];
-                gp += es;
-            }
+            for (int k = 0; k < 8; ++k) v[k] = w[k];
         }
     }
+}
+
+template <int AXIS>
+__device__ __forceinline__ void backward_uniform(const SubDev& sd, float* slot, int lane, float& x, float o[32],
+                                                 int exact) {
+    const float x_in = x;
+    const float R = sd.R, nF = sd.nF;
+    const float2 nS2 = make_float2(sd.nS, sd.nSR), R2 = make_float2(R, R), nF2 = make_float2(nF, nF);
+    uint32_t bad = 0;
+    float v[8], w[8];
+    load8<AXIS>(slot, 24, lane, v);
+#pragma unroll
+    for (int b8 = 3; b8 >= 0; --b8) {
+        if (b8 > 0) load8<AXIS>(slot, 8 * b8 - 8, lane, w);
+        float yr[8];
+#pragma unroll
+        for (int k = 0; k < 8; k += 2) {
+            const float2 q = __fmul2_rn(make_float2(v[k], v[k + 1]), R2);
+            yr[k] = q.x;
+            yr[k + 1] = q.y;
+        }
+        float t[8], a1[8];
+#pragma unroll
+        for (int k = 7; k >= 0; --k) {
+            // (t, a0) = (fma(-s, x, y), fma(-s/F, x, y/F))
+            const float2 ta = __ffma2_rn(nS2, make_float2(x, x), make_float2(v[k], yr[k]));
+            const float r0 = __fmaf_rn(ta.y, nF, ta.x);
+            x = __fmaf_rn(r0, R, ta.y);  // a1, carried on the chain
+            t[k] = ta.x;
+            a1[k] = x;
+            o[8 * b8 + k] = x;
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k += 2) {
+            const float2 a = make_float2(a1[k], a1[k + 1]);
+            const float2 r1 = __ffma2_rn(a, nF2, make_float2(t[k], t[k + 1]));
+            const float2 a2 = __ffma2_rn(r1, R2, a);  // exact quotients
+            bad |= (__float_as_uint(a.x) ^ __float_as_uint(a2.x)) | (__float_as_uint(a.y) ^ __float_as_uint(a2.y));
+        }
+        if (b8 > 0) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v[k] = w[k];
+        }
+    }
+    if (__any_sync(FULL, bad != 0) || exact) {
+        x = x_in;
+#pragma unroll
+        for (int e = 31; e >= 0; --e) {
+            x = div_rn(__fmaf_rn(sd.nS, x, *elem<AXIS>(slot, e, lane)), -nF, R);
+            o[e] = x;
+        }
+    }
+}
+
+// Back substitution over group g, from its top element down; the results replace the group's
+// values in its slot, from where one TMA store writes them back.
+template <int AXIS>
+__device__ __forceinline__ void backward_group(const SweepCtx& c, const SubDev& sd, float* slot, int g, int lane,
+                                               float& x, int exact) {
+    float o[32];
+    if ((sd.uni >> g) & 1u) backward_uniform<AXIS>(sd, slot, lane, x, o, exact);
+    else backward_full<AXIS>(c, slot, 32 * g, lane, x, o, exact);
+#pragma unroll
+    for (int b8 = 0; b8 < 4; ++b8) store8<AXIS>(slot, 8 * b8, lane, o + 8 * b8);
 }
 
 // y/z: rows of the end groups that hold boundary elements (j = 0 and j >= N-1) get b.
@@ -392,12 +464,23 @@ __device__ __forceinline__ void edge_rows(const SweepCtx& c, float* slot, int g,
     __syncwarp();
 }
 
-// One tile of parity Q: forward elimination as its groups land, back substitution from the top
-// group down, every finished group stored by TMA and its slot refilled with the next tile.
+// Warp roles.  Each compute warp owns B slots of 4 KB and walks its tiles: the forward
+// elimination waits for each group's box on full[g]; the back substitution leaves each group's
+// results in its slot and signals empty[g].  One producer thread issues every TMA copy: the first
+// tile of each compute warp, then for every signalled group the store of its results and, once that
+// store has read the slot, the load of the warp's next tile's group that takes the slot over.  Both
+// barriers complete once per tile, so tile k of a warp waits on parity k & 1.
+//
+// Slots: a tile of parity 0 keeps group g in slot g, a tile of parity 1 in slot B-1-g.  The back
+// substitution frees slots from the top group down, which is where the next tile's bottom groups
+// (the ones its forward elimination needs first) go: group B-1-g of tile k+1 reuses the slot of
+// group g of tile k.
+__host__ __device__ __forceinline__ int slot_index(int g, int q, int B) { return q ? B - 1 - g : g; }
+
 template <int AXIS, int Q>
-__device__ __forceinline__ bool run_tile(const LodArgs& a, const TileDesc& d, const TileDesc& dn, bool has_next,
-                                         float* buf, uint64_t* bars, uint32_t& ph, const float* sEFR, int Na) {
-    const int N = a.g.N, P = a.g.P;
+__device__ __forceinline__ bool run_tile(const LodArgs& a, const TileDesc& d, float* buf, uint64_t* full,
+                                         uint64_t* empty, const float* sEFR, int Na) {
+    const int N = a.g.N;
     const int B = (N + 31) >> 5;
     const int lane = threadIdx.x & 31;
     const SubDev& sd = a.sub[d.s];
@@ -406,96 +489,102 @@ __device__ __forceinline__ bool run_tile(const LodArgs& a, const TileDesc& d, co
     c.FR = sd.FRS;
     c.b = sd.b;
     c.dt = a.dt;
-    auto slot_of = [&](int g, int q) { return buf + (size_t)(q ? B - 1 - g : g) * kSlotFloats; };
-    uint32_t interior = 0, flagged = 0, special = 0;
+    uint32_t special = 0;
+    XReset xr{0, 0, c.b};
     if (AXIS == 0) {
-        interior = __ballot_sync(FULL, d.interior_lane);
-        flagged = __ballot_sync(FULL, d.flagged_lane);
-        special = ~interior & ~flagged;  // boundary lines: every group needs the reset
+        const bool sp = !d.flagged_lane && !d.interior_lane;
+        xr.lo = d.flagged_lane ? 1 : (d.interior_lane ? 2 : 0x7fffffff);
+        xr.hi = d.flagged_lane ? N - 2 : N - 3;
+        special = __ballot_sync(FULL, sp);  // boundary lines: every group needs the reset
     }
 
     float Y = c.b;
     for (int g = 0; g < B; ++g) {
-        if (!mbar_wait(bars + g, (ph >> g) & 1u, a.err, 1 + AXIS)) return false;
-        ph ^= 1u << g;
-        float* slot = slot_of(g, Q);
+        if (!mbar_wait(full + g, (uint32_t)Q, a.err, 1 + AXIS)) return false;
+        float* slot = buf + (size_t)slot_index(g, Q, B) * kSlotFloats;
         const bool edge = g == 0 || 32 * g + 31 > N - 3;
-        if (AXIS == 0) {
-            const uint32_t lines = edge ? 0xffffffffu : special;
-            if (lines) x_prepass(c, slot, g, N, lines, interior, flagged);
-        } else if (edge) {
-            edge_rows<AXIS>(c, slot, g, N, lane);
-        }
-        forward_group<AXIS>(c, slot, g, lane, Y);
+        const bool rs = AXIS == 0 && (edge || special != 0);
+        if (AXIS != 0 && edge) edge_rows<AXIS>(c, slot, g, N, lane);
+        if ((sd.uni >> g) & 1u) forward_uniform<AXIS>(slot, g, lane, Y, sd.nE, rs, xr);
+        else forward_group<AXIS>(c, slot, g, lane, Y, rs, xr);
     }
     float x = c.b;
-    // this lane's column in global memory (y/z): element 0 of its line, and the element stride
-    float* gcol = nullptr;
-    long long es = 0;
-    bool store_ok = false;
-    if (AXIS == 1) {
-        gcol = sd.p + d.c0 + lane + (long long)d.c2 * a.g.PN;
-        es = P;
-        store_ok = d.c0 + lane < P;
-    } else if (AXIS == 2) {
-        gcol = sd.p + d.c0 + lane;
-        es = a.g.PN;
-        store_ok = d.c0 + lane < a.g.PN;
-    }
     for (int g = B - 1; g >= 0; --g) {
-        float* slot = slot_of(g, Q);
-        backward_group<AXIS>(c, slot, g, N, lane, x, gcol, es, store_ok);
-        if (AXIS == 0) {
-            // the slot now holds the results: make them visible to the TMA store
-            fence_proxy_async();
-            __syncwarp();
-            if (lane == 0) {
-                box_store<AXIS>(a, d, g, slot);
-                bulk_commit();
-                if (has_next && g + 1 <= B - 1) {
-                    // the store of group g+1 has read its slot: refill it with the next tile
-                    bulk_wait_read<1>();
-                    box_load<AXIS>(a, dn, B - 2 - g, slot_of(g + 1, Q), bars + (B - 2 - g));
-                }
-            }
-            __syncwarp();
-        } else {
-            // every lane has read the slot: refill it with the next tile's group
-            __syncwarp();
-            if (lane == 0 && has_next) box_load<AXIS>(a, dn, B - 1 - g, slot, bars + (B - 1 - g));
-        }
-    }
-    if (AXIS == 0) {
-        if (lane == 0) {
-            bulk_wait_read<0>();
-            if (has_next) box_load<AXIS>(a, dn, B - 1, slot_of(0, Q), bars + (B - 1));
-        }
+        float* slot = buf + (size_t)slot_index(g, Q, B) * kSlotFloats;
+        backward_group<AXIS>(c, sd, slot, g, lane, x, a.exact);
+        // the slot now holds the results: make them visible to the TMA store, then hand it over
+        fence_proxy_async();
         __syncwarp();
+        if (lane == 0) mbar_arrive(empty + g);
     }
     return true;
 }
 
+// The producer of compute warp w (lane 0 of warp W + w) follows the same tiles: first tile's loads,
+// then per signalled group the store of its results and the refill of the slot of the group before
+// it (whose store has read the slot by then), as the compute warp frees them.
 template <int AXIS>
-__global__ void __launch_bounds__(256, 1) k_sweep(const __grid_constant__ LodArgs a) {
+__device__ void producer(const LodArgs& a, float* buf, uint64_t* full, uint64_t* empty, long long t, long long total,
+                         long long step, long long per_sub) {
+    const int B = (a.g.N + 31) >> 5;
+    TileDesc d = tile_coords<AXIS>(a, t, per_sub);
+    for (int g = 0; g < B; ++g) box_load<AXIS>(a, d, g, buf + (size_t)g * kSlotFloats, full + g);
+    for (int k = 0;; ++k) {
+        const int Q = k & 1;
+        const long long tn = t + step;
+        const bool has_next = tn < total;
+        const TileDesc dn = has_next ? tile_coords<AXIS>(a, tn, per_sub) : d;
+        for (int g = B - 1; g >= 0; --g) {
+            if (!mbar_wait1(empty + g, (uint32_t)Q, a.err, 8 + AXIS)) {
+                asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+                return;
+            }
+            float* slot = buf + (size_t)slot_index(g, Q, B) * kSlotFloats;
+            box_store<AXIS>(a, d, g, slot);
+            bulk_commit();
+            if (has_next && g + 1 <= B - 1) {
+                // the store of group g+1 has read its slot: refill it with the next tile
+                bulk_wait_read<1>();
+                box_load<AXIS>(a, dn, B - 2 - g, buf + (size_t)slot_index(g + 1, Q, B) * kSlotFloats,
+                               full + (B - 2 - g));
+            }
+        }
+        if (!has_next) break;
+        bulk_wait_read<0>();
+        box_load<AXIS>(a, dn, B - 1, buf + (size_t)slot_index(0, Q, B) * kSlotFloats, full + (B - 1));
+        t = tn;
+        d = dn;
+    }
+    // no bulk store may outlive the CTA's shared memory
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
+// blockDim = 2W warps: W <= kMaxComputeWarps compute warps, then their W producer warps.
+constexpr int kMaxComputeWarps = 4;
+template <int AXIS>
+__global__ void __launch_bounds__(64 * kMaxComputeWarps, 1) k_sweep(const __grid_constant__ LodArgs a) {
     extern __shared__ __align__(1024) unsigned char sm[];
     const Geom g = a.g;
     const int N = g.N, P = g.P;
     const int Na = (N + 31) & ~31;  // per substrate: E[Na] in shared memory
     const int B = (N + 31) >> 5;
-    const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int W = blockDim.x >> 6, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // 1024-byte aligned slots first (the x boxes use the 128-byte swizzle), then tables, barriers
     const uint32_t base = smem_u32(sm);
     unsigned char* sm1 = sm + ((1024 - (base & 1023)) & 1023);
-    float* buf = reinterpret_cast<float*>(sm1) + (size_t)warp * B * kSlotFloats;
-    float* sEFR = reinterpret_cast<float*>(sm1 + (size_t)warps * B * kSlotFloats * 4);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sm1 + (size_t)warps * B * kSlotFloats * 4 +
-                                                 align128(a.nsub * Na * 4)) + warp * 32;
+    float* slots = reinterpret_cast<float*>(sm1);
+    float* sEFR = reinterpret_cast<float*>(sm1 + (size_t)W * B * kSlotFloats * 4);
+    uint64_t* full = reinterpret_cast<uint64_t*>(sm1 + (size_t)W * B * kSlotFloats * 4 + align128(a.nsub * Na * 4));
+    uint64_t* empty = full + W * 32;
     for (int i = threadIdx.x; i < a.nsub * Na; i += blockDim.x) {
         const int s = i / Na, j = i - s * Na;
         // E of the elements the reference's recurrences update; 0 elsewhere (identity)
         sEFR[i] = (j >= 1 && j <= N - 2) ? a.sub[s].EFR[j] : 0.f;
     }
-    if (lane < B) mbar_init(bars + lane, 1u);
+    for (int i = threadIdx.x; i < W * 32; i += blockDim.x) {
+        mbar_init(full + i, 1u);
+        mbar_init(empty + i, 1u);
+    }
     fence_mbar_init();
     __syncthreads();
 
@@ -504,30 +593,25 @@ __global__ void __launch_bounds__(256, 1) k_sweep(const __grid_constant__ LodArg
     else if (AXIS == 1) per_sub = (long long)((P + 31) / 32) * N;
     else per_sub = (g.PN + 31) / 32;
     const long long total = per_sub * a.nsub;
-    const long long step = (long long)gridDim.x * warps;
-    long long t = (long long)blockIdx.x * warps + warp;
-    if (t >= total) return;
+    const long long step = (long long)gridDim.x * W;
 
-    TileDesc d = tile_desc<AXIS>(a, t, per_sub);
-    if (lane == 0)
-        for (int gi = 0; gi < B; ++gi) box_load<AXIS>(a, d, gi, buf + (size_t)gi * kSlotFloats, bars + gi);
-    __syncwarp();
-    uint32_t ph = 0;
-    int q = 0;
-    for (;;) {
-        const long long tn = t + step;
-        const bool has_next = tn < total;
-        const TileDesc dn = has_next ? tile_desc<AXIS>(a, tn, per_sub) : d;
-        const bool ok = q == 0 ? run_tile<AXIS, 0>(a, d, dn, has_next, buf, bars, ph, sEFR, Na)
-                               : run_tile<AXIS, 1>(a, d, dn, has_next, buf, bars, ph, sEFR, Na);
-        if (!ok || !has_next) break;
-        t = tn;
-        d = dn;
-        q ^= 1;
+    if (warp >= W) {
+        const int w = warp - W;
+        const long long t = (long long)blockIdx.x * W + w;
+        if (lane == 0 && t < total)
+            producer<AXIS>(a, slots + (size_t)w * B * kSlotFloats, full + w * 32, empty + w * 32, t, total, step, per_sub);
+        return;
     }
-    // no bulk store may outlive the CTA's shared memory
-    if (lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
-    __syncwarp();
+    float* buf = slots + (size_t)warp * B * kSlotFloats;
+    uint64_t* fb = full + warp * 32;
+    uint64_t* eb = empty + warp * 32;
+    int k = 0;
+    for (long long t = (long long)blockIdx.x * W + warp; t < total; t += step, ++k) {
+        const TileDesc d = tile_desc<AXIS>(a, t, per_sub);
+        const bool ok = (k & 1) ? run_tile<AXIS, 1>(a, d, buf, fb, eb, sEFR, Na)
+                                : run_tile<AXIS, 0>(a, d, buf, fb, eb, sEFR, Na);
+        if (!ok) break;
+    }
 }
 
 // Markstein division against IEEE division on random operands in the sweeps' range.
@@ -686,7 +770,11 @@ gell_status lod_solver(gell_ctx* c, int sub, int substeps) {
     int ns = 0;
     for (int s = s0; s < s1; ++s, ++ns) {
         const Substrate& S = c->subs[s];
-        const SubDev sd{S.p, S.rate, S.line_flag, S.EF, S.FRS, S.s.boundary, S.side};
+        const int N = c->g.N;
+        const float R = S.conv_R;
+        const SubDev sd{S.p,         S.rate,  S.line_flag,       S.EF,         S.FRS, S.s.boundary,
+                        S.side,      S.uniform_groups,           -S.E[N - 2],  -S.side,
+                        -(S.side * R), -S.F[N - 2],              R};
         ax.sub[ns] = ay.sub[ns] = az.sub[ns] = sd;
         ax.tm[ns] = S.tmap[0];
         ay.tm[ns] = S.tmap[1];
@@ -697,16 +785,17 @@ gell_status lod_solver(gell_ctx* c, int sub, int substeps) {
         a->g = c->g;
         a->dt = c->P.diffusion_dt;
         a->err = c->dev_err;
+        a->exact = c->exact_chain ? 1 : 0;
     }
     const int N = c->g.N;
     const int B = (N + 31) / 32;
     const int Na = (N + 31) & ~31;
     const int smem_cap = 227 * 1024;
-    const int fixed = 1024 + align128(ns * Na * 4) + 16 * 32 * 8;
+    const int fixed = 1024 + align128(ns * Na * 4) + 2 * 8 * 32 * 8;
     int w = (smem_cap - fixed) / (B * kSlotFloats * 4);
-    w = w > 8 ? 8 : w;
+    w = w > kMaxComputeWarps ? kMaxComputeWarps : w;
     if (w < 1) return fail(c, GELL_ERR_UNSUPPORTED, "grid edge too large for the shared-memory line tiles");
-    const int smem = 1024 + w * B * kSlotFloats * 4 + align128(ns * Na * 4) + align128(w * 32 * 8);
+    const int smem = 1024 + w * B * kSlotFloats * 4 + align128(ns * Na * 4) + 2 * w * 32 * 8;
     static bool configured = false;
     if (!configured) {
         GELL_CUDA(c, cudaFuncSetAttribute(k_sweep<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
@@ -737,9 +826,9 @@ gell_status lod_solver(gell_ctx* c, int sub, int substeps) {
     sa.dt = c->P.diffusion_dt;
     for (int k = 0; k < substeps; ++k) {
         GELL_KERNEL(c, "k_source_lines", k_source_lines<<<num_sms() * 8, 256, 0, c->stream>>>(sa));
-        GELL_KERNEL(c, "k_sweep_x", k_sweep<0><<<gx, w * 32, smem, c->stream>>>(ax));
-        GELL_KERNEL(c, "k_sweep_y", k_sweep<1><<<gy, w * 32, smem, c->stream>>>(ay));
-        GELL_KERNEL(c, "k_sweep_z", k_sweep<2><<<gz, w * 32, smem, c->stream>>>(az));
+        GELL_KERNEL(c, "k_sweep_x", k_sweep<0><<<gx, w * 64, smem, c->stream>>>(ax));
+        GELL_KERNEL(c, "k_sweep_y", k_sweep<1><<<gy, w * 64, smem, c->stream>>>(ay));
+        GELL_KERNEL(c, "k_sweep_z", k_sweep<2><<<gz, w * 64, smem, c->stream>>>(az));
     }
     return GELL_OK;
 }

@@ -243,6 +243,12 @@ gell_status gell_selftest_division(gell_ctx* ctx, int64_t samples, uint64_t seed
 gell_status gell_sort_keys_noalloc(const int32_t* keys, int32_t* sorted_keys, int32_t* perm, int n,
                                    int key_bits, void* stream);
 
+/* Options (none has a reference counterpart).  GELL_OPT_EXACT_CHAIN = 1 makes the LOD back
+ * substitution run the exact division chain for every group instead of the speculative chain that
+ * is checked against it; results are identical either way, this only makes the exact path testable. */
+enum { GELL_OPT_EXACT_CHAIN = 1 };
+gell_status gell_set_option(gell_ctx* ctx, int option, int64_t value);
+
 /* Number of kernels this context has launched (always counted). */
 gell_status gell_launch_count(gell_ctx* ctx, int64_t* count);
 

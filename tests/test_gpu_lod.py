@@ -37,12 +37,13 @@ def test_ef_prefactor_bit_exact(N):
             assert bits_equal(E, oE) and bits_equal(F, oF)
 
 
-@pytest.mark.parametrize("N,k", [(32, 1), (32, 10), (37, 3), (64, 2)])
+@pytest.mark.parametrize("N,k", [(32, 1), (32, 10), (37, 3), (64, 2), (100, 3), (131, 2)])
 def test_lod_bit_exact_one_cell_per_voxel(N, k):
+    """N >= 100 reaches the groups whose Thomas factors have converged (uniform-group path)."""
     length = 10.0
     cells = one_per_voxel(N, length, seed=N, lo=N // 4, hi=N // 4 + N // 2)
     field = random_field(N, seed=7)
-    with make_sim(N, length, subs=("o2", "drug")) as sim:
+    with make_sim(N, length, cap=max(65536, len(cells)), subs=("o2", "drug")) as sim:
         sim.set_field(0, field)
         sim.set_field(1, field * 0.03)
         sim.import_cells(cells)
@@ -172,3 +173,27 @@ def test_markstein_division_matches_ieee():
     with make_sim(16, 10.0, cap=16) as sim:
         assert sim.selftest_division(1 << 26, seed=11) == 0
         assert sim.selftest_division(1 << 26, seed=12) == 0
+
+
+@pytest.mark.parametrize("N", [100, 160])
+def test_exact_chain_option_gives_identical_fields(N):
+    """The back substitution's speculative chain is verified against the exact one and redone
+    where they differ; forcing the exact chain everywhere must give the same bits."""
+    length = 10.0
+    cells = one_per_voxel(N, length, seed=N + 1, lo=N // 4, hi=N // 4 + N // 2)
+    field = random_field(N, seed=17)
+    out = []
+    for exact in (False, True):
+        with make_sim(N, length, cap=max(65536, len(cells)), subs=("o2", "drug")) as sim:
+            sim.set_exact_chain(exact)
+            sim.set_field(0, field)
+            sim.set_field(1, field * 0.03)
+            sim.import_cells(cells)
+            sim.PreLOD()
+            sim.LODsolver(3)
+            out.append((sim.field(0), sim.field(1)))
+    for a, b in zip(out[0], out[1]):
+        assert bits_equal(a, b)
+    rate = ol.prelod(cells, N, length, -10.0)
+    E, F = ol.mesh_init(N, length, 1e5, 0.1, 0.01)
+    assert bits_equal(out[1][0], ol.lod_substeps(field, rate, E, F, N, 0.01, 38.0, 3))
