@@ -31,11 +31,19 @@ struct BioParams {
     float dur_pre2post, dur_post2q;
 };
 
-// Cell::Volume_update (include/Cells.cuh:91-143).  Vx' = fma(Vx, 1 - dt*rx, (rx*dt)*Vx_0) with
-// 1 - dt*rx and rx*dt rounded once each, V = (Vf + Vns) + Vcs, r = cbrt-by-pow in double.
-__device__ __forceinline__ float relax(float v, float rx, float v0, float dt) {
+// Cell::Volume_update (include/Cells.cuh:91-143): Vx' = Vx*(1 - dt*rx) + (rx*dt)*Vx_0 with the
+// reference's device rounding.  1 - dt*rx and rx*dt are rounded once each; the fluid compartment,
+// whose target V*ff varies per cell, fuses Vf*(1 - dt*rf) into the sum, while the nuclear and
+// cytoplasmic compartments, whose targets are per-phase constants, fuse (rx*dt)*Vx_0 instead
+// (measured against the reference's own device build on every phase).  V = (Vf + Vns) + Vcs,
+// r = cbrt-by-pow in double.
+__device__ __forceinline__ float relax_fluid(float v, float rx, float v0, float dt) {
     const float k = __fsub_rn(1.f, __fmul_rn(dt, rx));
     return __fmaf_rn(v, k, __fmul_rn(__fmul_rn(rx, dt), v0));
+}
+__device__ __forceinline__ float relax_const_target(float v, float rx, float v0, float dt) {
+    const float k = __fsub_rn(1.f, __fmul_rn(dt, rx));
+    return __fmaf_rn(__fmul_rn(rx, dt), v0, __fmul_rn(v, k));
 }
 
 __device__ void volume_update(int ph, float& V, float& Vf, float& Vcs, float& Vns, float& r) {
@@ -68,9 +76,9 @@ __device__ void volume_update(int ph, float& V, float& Vf, float& Vcs, float& Vn
     }
     const float Vf_0 = __fmul_rn(V, ff);
     const float Vcs_0 = __fmul_rn(Vns_0, 3.615f);
-    Vf = relax(Vf, rf, Vf_0, dt);
-    Vns = relax(Vns, rns, Vns_0, dt);
-    Vcs = relax(Vcs, rcs, Vcs_0, dt);
+    Vf = relax_fluid(Vf, rf, Vf_0, dt);
+    Vns = relax_const_target(Vns, rns, Vns_0, dt);
+    Vcs = relax_const_target(Vcs, rcs, Vcs_0, dt);
     V = __fadd_rn(__fadd_rn(Vf, Vns), Vcs);
     r = (float)pow(0.23873241 * (double)V, 1.0 / 3);
 }

@@ -423,12 +423,18 @@ void go_fm_update(go_cell* cells, int n, const go_params* P, int* keys, int* per
  * The reference's host build (g++) rounds every operation; its device build (nvcc) fuses the
  * outer multiply-add.  mode GO_VOL_HOST: every operation rounded.  GO_VOL_DEVICE:
  * fma(Vx, 1 - dt*rx, (rx*dt)*Vx_0) with 1 - dt*rx and rx*dt rounded once each.
- * GO_VOL_DEVICE_FUSED: the inner 1 - dt*rx fused as well.  r from the double-precision pow. */
-static int g_vol_mode = GO_VOL_DEVICE;
+ * GO_VOL_DEVICE_FUSED: the inner 1 - dt*rx fused as well.  GO_VOL_DEVICE_SWAP(_FUSED): the other
+ * product fused, fma(rx*dt, Vx_0, Vx*(1 - dt*rx)).  GO_VOL_DEVICE_REF: what the reference's device
+ * build does, found by running it on every phase: the fluid compartment (target V*ff, per cell)
+ * as GO_VOL_DEVICE, the nuclear and cytoplasmic ones (per-phase constant targets) as
+ * GO_VOL_DEVICE_SWAP.  r from the double-precision pow. */
+static int g_vol_mode = GO_VOL_DEVICE_REF;
 void go_set_volume_mode(int mode) { g_vol_mode = mode; }
 static inline float relax(float v, float rx, float v0, float dt, int mode) {
     if (mode == GO_VOL_HOST) return v * (1.f - dt * rx) + rx * dt * v0;
-    float k = mode == GO_VOL_DEVICE_FUSED ? fmaf(-dt, rx, 1.f) : 1.f - dt * rx;
+    const int fused = mode == GO_VOL_DEVICE_FUSED || mode == GO_VOL_DEVICE_SWAP_FUSED;
+    const float k = fused ? fmaf(-dt, rx, 1.f) : 1.f - dt * rx;
+    if (mode == GO_VOL_DEVICE_SWAP || mode == GO_VOL_DEVICE_SWAP_FUSED) return fmaf(rx * dt, v0, v * k);
     return fmaf(v, k, rx * dt * v0);
 }
 void go_volume_update_mode(go_cell* c, int mode) {
@@ -463,13 +469,19 @@ void go_volume_update_mode(go_cell* c, int mode) {
     }
     float Vf_0 = c->V * ff;
     float Vcs_0 = Vns_0 * 3.615f;
-    c->Vf = relax(c->Vf, rf, Vf_0, dt, mode);
-    c->Vns = relax(c->Vns, rns, Vns_0, dt, mode);
-    c->Vcs = relax(c->Vcs, rcs, Vcs_0, dt, mode);
+    const int mf = mode == GO_VOL_DEVICE_REF ? GO_VOL_DEVICE : mode;
+    const int mc = mode == GO_VOL_DEVICE_REF ? GO_VOL_DEVICE_SWAP : mode;
+    c->Vf = relax(c->Vf, rf, Vf_0, dt, mf);
+    c->Vns = relax(c->Vns, rns, Vns_0, dt, mc);
+    c->Vcs = relax(c->Vcs, rcs, Vcs_0, dt, mc);
     c->V = c->Vf + c->Vns + c->Vcs;
     c->r = (float)pow(0.23873241 * (double)c->V, 1.0 / 3);
 }
 void go_volume_update(go_cell* c) { go_volume_update_mode(c, g_vol_mode); }
+void go_volume_update_modes(go_cell* c, int n, int mode) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) go_volume_update_mode(c + i, mode);
+}
 
 /* include/Cells.cuh:69-71 */
 void go_radius_update(go_cell* c) { c->r = (float)pow(0.23873241 * (double)c->V, 1.0 / 3); }

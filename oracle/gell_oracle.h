@@ -86,10 +86,12 @@ void go_move(go_cell* cells, int n, const go_params* P);
 void go_fm_update(go_cell* cells, int n, const go_params* P, int* keys, int* perm, int* s, int* e);
 
 /* ---- cell model (include/Cells.cuh) ---- */
-enum { GO_VOL_HOST = 0, GO_VOL_DEVICE = 1, GO_VOL_DEVICE_FUSED = 2 };
+enum { GO_VOL_HOST = 0, GO_VOL_DEVICE = 1, GO_VOL_DEVICE_FUSED = 2, GO_VOL_DEVICE_SWAP = 3, GO_VOL_DEVICE_SWAP_FUSED = 4,
+       GO_VOL_DEVICE_REF = 5 };
 void go_volume_update(go_cell* c);                                  /* :91-143 */
 void go_volume_update_mode(go_cell* c, int mode);
 void go_set_volume_mode(int mode);
+void go_volume_update_modes(go_cell* c, int n, int mode);           /* n cells, one mode */
 void go_radius_update(go_cell* c);                                  /* :69-71 */
 int go_phase_update(go_cell* c, float rnd, float o2, const go_params* P); /* :145-223 */
 void go_random_vect(float u, float v, float out[3]);                /* RandomFunctions.cuh:23-31 */

@@ -81,6 +81,24 @@ void gref_volume_update(Cell* c) { c->Volume_update(); }
 int gref_phase_update(Cell* c, float rnd, float o2) { return c->Phase_update_ki67adv(rnd, o2) ? 1 : 0; }
 void gref_radius_update(Cell* c) { c->Radius_update(); }
 
+// ---- the same Cell member function compiled for and run on the GPU
+static __global__ void gref_k_volume(Cell* c, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) c[i].Volume_update();
+}
+int gref_volume_update_device(Cell* host, int n) {
+    Cell* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, sizeof(Cell) * (size_t)n);
+    if (e == cudaSuccess) e = cudaMemcpy(d, host, sizeof(Cell) * (size_t)n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        gref_k_volume<<<(n + 255) / 256, 256>>>(d, n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(host, d, sizeof(Cell) * (size_t)n, cudaMemcpyDeviceToHost);
+    if (d) cudaFree(d);
+    return (int)e;
+}
+
 // ---- the reference's device state: meshes, cells, RNG (Main.cu:63-95)
 void* gref_create(float conc, float D, float decay) {
     GRef* g = new GRef;

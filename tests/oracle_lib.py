@@ -19,7 +19,8 @@ P = ctypes.c_void_p
 I = ctypes.c_int
 F = ctypes.c_float
 
-GO_VOL_HOST, GO_VOL_DEVICE, GO_VOL_DEVICE_FUSED = 0, 1, 2
+GO_VOL_HOST, GO_VOL_DEVICE, GO_VOL_DEVICE_FUSED, GO_VOL_DEVICE_SWAP, GO_VOL_DEVICE_SWAP_FUSED = 0, 1, 2, 3, 4
+GO_VOL_DEVICE_REF = 5
 
 
 class GoParams(ctypes.Structure):
@@ -70,6 +71,7 @@ def lib() -> ctypes.CDLL:
         L.go_volume_update.argtypes = [P]
         L.go_volume_update_mode.argtypes = [P, I]
         L.go_set_volume_mode.argtypes = [I]
+        L.go_volume_update_modes.argtypes = [P, I, I]
         L.go_radius_update.argtypes = [P]
         L.go_phase_update.argtypes = [P, F, F, P]
         L.go_phase_update.restype = I

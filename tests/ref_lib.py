@@ -43,6 +43,8 @@ def lib(name: str) -> ctypes.CDLL:
         for f in ("gref_get_field", "gref_set_field", "gref_get_rate", "gref_set_rate"):
             getattr(L, f).argtypes = [P, P]
         L.gref_get_ef.argtypes = [P, P, P]
+        L.gref_volume_update_device.argtypes = [P, ctypes.c_int]
+        L.gref_volume_update_device.restype = ctypes.c_int
         for f in ("gref_time_fm", "gref_time_prelod", "gref_time_lod"):
             getattr(L, f).argtypes = [P, ctypes.c_int, ctypes.c_int]
             getattr(L, f).restype = ctypes.c_float

@@ -164,3 +164,34 @@ def test_birth_counts_chi_squared_over_seeds():
         # 1000 degrees of freedom: mean 1000, sd ~45; reject beyond ~5 sd
         assert 780 < chi2 < 1230, (chi2, obs.mean(), mean)
         assert abs(obs.mean() - mean) < 5 * np.sqrt(var / len(obs))
+
+
+@pytest.mark.skipif(not ref_lib.available("t32"), reason="reference build oracle/_ref missing")
+def test_volume_update_contraction_vs_reference_device():
+    """Cell::Volume_update as the reference's device build computes it (include/Cells.cuh:91-143),
+    on 2^20 random cells over all phases, against the oracle's restatements of the possible
+    multiply-add fusions.  The one the kernels use (GO_VOL_DEVICE_REF) must match every bit."""
+    n = 1 << 20
+    rng = np.random.Generator(np.random.Philox(5))
+    c = np.zeros(n, CELL_DTYPE)
+    c["sign"] = 1
+    c["phase"] = rng.integers(0, 6, n)
+    c["V"] = rng.uniform(100, 6000, n).astype(np.float32)
+    c["Vf"] = rng.uniform(0, 4000, n).astype(np.float32)
+    c["Vns"] = rng.uniform(0, 600, n).astype(np.float32)
+    c["Vcs"] = rng.uniform(0, 2000, n).astype(np.float32)
+    dev = c.copy()
+    assert ref_lib.lib("t32").gref_volume_update_device(dev.ctypes.data, n) == 0
+    L = ol.lib()
+    res = {}
+    for name, mode in (("device", ol.GO_VOL_DEVICE), ("device_fused", ol.GO_VOL_DEVICE_FUSED),
+                       ("swap", ol.GO_VOL_DEVICE_SWAP), ("swap_fused", ol.GO_VOL_DEVICE_SWAP_FUSED),
+                       ("reference", ol.GO_VOL_DEVICE_REF)):
+        o = c.copy()
+        L.go_volume_update_modes(o.ctypes.data, n, mode)
+        same = np.ones(n, bool)
+        for f in ("Vf", "Vns", "Vcs", "V"):
+            same &= o[f].view(np.uint32) == dev[f].view(np.uint32)
+        res[name] = float(same.mean())
+    print("Volume_update bit-match with the reference device build:", res)
+    assert res["reference"] == 1.0

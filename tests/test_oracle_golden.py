@@ -79,7 +79,7 @@ def test_volume_update_device_semantics_close(gold):
     L = ol.lib()
     cells = cells_of(gold["model_in"])
     for n in range(len(cells)):
-        L.go_volume_update_mode(cells[n:n + 1].ctypes.data, ol.GO_VOL_DEVICE)
+        L.go_volume_update_mode(cells[n:n + 1].ctypes.data, ol.GO_VOL_DEVICE_REF)
     ref = cells_of(gold["volume_out"])
     for f in ("V", "Vf", "Vcs", "Vns", "r"):
         np.testing.assert_allclose(cells[f], ref[f], rtol=2e-6, atol=1e-4)
