@@ -93,40 +93,46 @@ __global__ void __launch_bounds__(256) k_force_move(MechArgs a) {
     const int3 b = find_bin(pr.x, pr.y, pr.z, a.g.len);
     float fx = 0.f, fy = 0.f, fz = 0.f;
     float thres = a.max_dist;
-    for (int xi = b.x - 1; xi <= b.x + 1; ++xi) {
-        for (int yi = b.y - 1; yi <= b.y + 1; ++yi) {
-            for (int zi = b.z - 1; zi <= b.z + 1; ++zi) {
-                if (!inside(xi, yi, zi, N)) continue;
-                const int4 e = a.bins[xi + (long long)yi * N + zi * NN];
-                if (e.z != a.epoch) continue;
-                for (int j = e.x; j <= e.y; ++j) {
-                    if (!a.cur.sign[j]) continue;
-                    const float4 q = a.cur.posr[j];
-                    const float dx = __fsub_rn(pr.x, q.x);
-                    const float dy = __fsub_rn(pr.y, q.y);
-                    const float dz = __fsub_rn(pr.z, q.z);
-                    const float ss = __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
-                    const float d = __fsqrt_rn(__double2float_rn(__dadd_rn((double)ss, 0.0001)));
-                    if (d >= thres) continue;
-                    const float rs = __fadd_rn(q.w, pr.w);
-                    const float R = rs > 0.01f ? rs : 0.01f;
-                    thres = __double2float_rn(__dmul_rn((double)R, a.ra_ratio));
-                    if (d >= thres) continue;
-                    float cr = 0.f, ca = 0.f;
-                    if (d <= R) {
-                        const float t = __fsub_rn(1.f, __fdiv_rn(d, R));
-                        cr = __fmul_rn(a.cccr, __fdiv_rn(__fmul_rn(t, t), d));
-                    }
-                    if (d <= thres) {
-                        const float t = __fsub_rn(1.f, __fdiv_rn(d, thres));
-                        ca = __fmul_rn(a.ccca, __fdiv_rn(__fmul_rn(t, t), d));
-                    }
-                    const float cf = __fsub_rn(cr, ca);
-                    fx = __fmaf_rn(dx, cf, fx);
-                    fy = __fmaf_rn(dy, cf, fy);
-                    fz = __fmaf_rn(dz, cf, fz);
-                }
+    // d >= thres is certain when |dp|^2 + 0.0001 (in double) exceeds thres^2 by a relative margin
+    // far above the roundings between it and d: such candidates skip the square root.
+    double thr_hi = (double)thres * (double)thres * (1.0 + 0x1p-20);
+    // the 27 bins in the reference's order: xi outer, then yi, then zi
+#pragma unroll 1
+    for (int o = 0; o < 27; ++o) {
+        const int xi = b.x - 1 + o / 9, yi = b.y - 1 + (o / 3) % 3, zi = b.z - 1 + o % 3;
+        if (!inside(xi, yi, zi, N)) continue;
+        const int4 e = a.bins[xi + (long long)yi * N + zi * NN];
+        if (e.z != a.epoch) continue;
+#pragma unroll 1
+        for (int j = e.x; j <= e.y; ++j) {
+            if (!a.cur.sign[j]) continue;
+            const float4 q = a.cur.posr[j];
+            const float dx = __fsub_rn(pr.x, q.x);
+            const float dy = __fsub_rn(pr.y, q.y);
+            const float dz = __fsub_rn(pr.z, q.z);
+            const float ss = __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
+            const double x = __dadd_rn((double)ss, 0.0001);
+            if (x > thr_hi) continue;
+            const float d = __fsqrt_rn(__double2float_rn(x));
+            if (d >= thres) continue;
+            const float rs = __fadd_rn(q.w, pr.w);
+            const float R = rs > 0.01f ? rs : 0.01f;
+            thres = __double2float_rn(__dmul_rn((double)R, a.ra_ratio));
+            thr_hi = (double)thres * (double)thres * (1.0 + 0x1p-20);
+            if (d >= thres) continue;
+            float cr = 0.f, ca = 0.f;
+            if (d <= R) {
+                const float t = __fsub_rn(1.f, __fdiv_rn(d, R));
+                cr = __fmul_rn(a.cccr, __fdiv_rn(__fmul_rn(t, t), d));
             }
+            if (d <= thres) {
+                const float t = __fsub_rn(1.f, __fdiv_rn(d, thres));
+                ca = __fmul_rn(a.ccca, __fdiv_rn(__fmul_rn(t, t), d));
+            }
+            const float cf = __fsub_rn(cr, ca);
+            fx = __fmaf_rn(dx, cf, fx);
+            fy = __fmaf_rn(dy, cf, fy);
+            fz = __fmaf_rn(dz, cf, fz);
         }
     }
     const float h = a.half_dt;
