@@ -11,7 +11,8 @@ both substrates.
   components cell-updates/s of FM_update + PreLOD alone, voxel-updates/s of the LOD substeps
              (voxels x substrates x substeps / LOD device time)
   e2e        the same rate through the C ABI with host buffers: every step imports the cells
-             from pinned host memory and exports them back, copies inside the timed region
+             from pinned host memory and exports them back, copies inside the timed region; the
+             copies are the ABI's queued transfers, which overlap the LOD substeps
   roofline   the kernel with the largest device time in the timed region, against HBM
 
 `--impl reference` times the CPU restatement of the reference's hot path (the oracle, OpenMP on
@@ -236,9 +237,12 @@ def run_gell(args, rank, world, local_rank):
     torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(ke):
-        sim.import_cells(host)
+        # the step's cells in from pinned host memory and its result out: queued transfers that
+        # overlap the LOD substeps (which do not use the cells)
+        sim.import_cells_async(host)
         step()
-        sim.export_cells(host)
+        sim.export_cells_async(host)
+    sim.wait_transfers()
     e1.record(stream)
     torch.cuda.synchronize()
     t_e2e = e0.elapsed_time(e1)

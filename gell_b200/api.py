@@ -113,6 +113,9 @@ def load_library() -> ctypes.CDLL:
     L.gell_cells_import.argtypes = [P, P, ctypes.c_int, ctypes.c_int]
     L.gell_cells_export.argtypes = [P, P, ctypes.c_int, P, ctypes.c_int]
     L.gell_cell_count.argtypes = [P, P]
+    L.gell_cells_import_async.argtypes = [P, P, ctypes.c_int]
+    L.gell_cells_export_async.argtypes = [P, P, ctypes.c_int, P]
+    L.gell_wait_transfers.argtypes = [P]
     L.gell_field_import.argtypes = [P, ctypes.c_int, P, ctypes.c_int]
     L.gell_field_export.argtypes = [P, ctypes.c_int, P, ctypes.c_int]
     L.gell_fm_update.argtypes = [P]
@@ -138,7 +141,8 @@ def load_library() -> ctypes.CDLL:
                  "gell_field_export", "gell_fm_update", "gell_prelod", "gell_lod_solver",
                  "gell_cell_birth", "gell_cell_death", "gell_mechanics_step", "gell_sync",
                  "gell_debug_dump", "gell_profile_enable", "gell_profile_read", "gell_launch_count",
-                 "gell_selftest_division", "gell_set_option"):
+                 "gell_selftest_division", "gell_set_option", "gell_cells_import_async",
+                 "gell_cells_export_async", "gell_wait_transfers"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
@@ -231,6 +235,26 @@ class Simulation:
         self._check(self.lib.gell_cells_export(self.h, P(_ptr(out)), len(out), ctypes.byref(cnt), 0),
                     "gell_cells_export")
         return out[:cnt.value]
+
+    def import_cells_async(self, cells: np.ndarray) -> None:
+        """Queued import from host memory (pinned for overlap); `cells` must stay unchanged until
+        the transfer has finished (sync(), or wait_transfers() in stream order)."""
+        if cells.dtype != CELL_DTYPE:
+            raise TypeError("cells must have gell_b200.CELL_DTYPE")
+        n = len(cells)
+        self._check(self.lib.gell_cells_import_async(self.h, P(_ptr(cells) if n else 0), n),
+                    "gell_cells_import_async")
+
+    def export_cells_async(self, out: np.ndarray) -> int:
+        """Queued export into host memory `out`; valid after sync().  Returns the count."""
+        cnt = ctypes.c_int()
+        self._check(self.lib.gell_cells_export_async(self.h, P(_ptr(out)), len(out), ctypes.byref(cnt)),
+                    "gell_cells_export_async")
+        return cnt.value
+
+    def wait_transfers(self) -> None:
+        """Make the context's stream wait for every queued transfer (the host does not block)."""
+        self._check(self.lib.gell_wait_transfers(self.h), "gell_wait_transfers")
 
     def export_cells_device(self, out_tensor) -> int:
         """Write the cells as 72-byte records into a CUDA uint8 tensor; returns the count."""

@@ -192,6 +192,9 @@ static void free_all(gell_ctx* c) {
     for (auto& p : c->prof) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
     for (auto e : c->ev_pool) cudaEventDestroy(e);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    if (c->xfer) cudaStreamDestroy(c->xfer);
+    if (c->cells_ev) cudaEventDestroy(c->cells_ev);
+    if (c->xfer_ev) cudaEventDestroy(c->xfer_ev);
 }
 
 gell_status gell_create(const gell_params* params, gell_ctx** out) {
@@ -233,6 +236,13 @@ gell_status gell_create(const gell_params* params, gell_ctx** out) {
         return GELL_ERR_CUDA;
     }
     c->stream = c->own_stream;
+    if (cudaStreamCreateWithFlags(&c->xfer, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->cells_ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->xfer_ev, cudaEventDisableTiming) != cudaSuccess) {
+        free_all(c);
+        delete c;
+        return GELL_ERR_CUDA;
+    }
     for (int b = 0; b < 2; ++b) {
         A((void**)&c->sign.b[b], cap);
         A((void**)&c->mesh.b[b], cap * 4);
@@ -298,6 +308,7 @@ gell_status gell_set_stream(gell_ctx* c, void* stream) {
 gell_status gell_sync(gell_ctx* c) {
     if (!c) return GELL_ERR_INVALID_ARG;
     GELL_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (c->xfer_pending) GELL_CUDA(c, cudaStreamSynchronize(c->xfer));
     int herr = 0;
     GELL_CUDA(c, cudaMemcpy(&herr, c->dev_err, 4, cudaMemcpyDeviceToHost));
     if (herr) return fail(c, GELL_ERR_TIMEOUT, "a bounded device wait gave up (code " + std::to_string(herr) + ")");
@@ -445,8 +456,25 @@ gell_status gell_substrate_add(gell_ctx* c, const gell_substrate* s, int* index_
     return GELL_OK;
 }
 
+}  // extern "C"
+
+// Work on `stream` that uses the cells first waits for the queued transfers, and afterwards marks
+// the point the next queued transfer has to wait for.
+static gell_status cells_begin(gell_ctx* c) {
+    if (c->xfer_pending) GELL_CUDA(c, cudaStreamWaitEvent(c->stream, c->xfer_ev, 0));
+    return GELL_OK;
+}
+static gell_status cells_end(gell_ctx* c, gell_status st) {
+    if (st != GELL_OK) return st;
+    GELL_CUDA(c, cudaEventRecord(c->cells_ev, c->stream));
+    return GELL_OK;
+}
+
+extern "C" {
+
 gell_status gell_cells_import(gell_ctx* c, const gell_cell* cells, int n, int on_device) {
     if (!c || (n > 0 && !cells) || n < 0) return GELL_ERR_INVALID_ARG;
+    if (gell_status b = cells_begin(c)) return b;
     if (n > c->cap) return fail(c, GELL_ERR_CAPACITY, "more cells than max_cell_num");
     const gell_cell* src = cells;
     if (!on_device && n > 0) {
@@ -460,12 +488,13 @@ gell_status gell_cells_import(gell_ctx* c, const gell_cell* cells, int n, int on
     c->n = n;
     c->sorted_valid = false;
     c->rate_valid = false;
-    return GELL_OK;
+    return cells_end(c, GELL_OK);
 }
 
 gell_status gell_cells_export(gell_ctx* c, gell_cell* cells, int capacity, int* n_out, int on_device) {
     if (!c || (c->n > 0 && !cells)) return GELL_ERR_INVALID_ARG;
     if (capacity < c->n) return fail(c, GELL_ERR_CAPACITY, "export buffer too small");
+    if (gell_status b = cells_begin(c)) return b;
     int n = c->n;
     if (n > 0) {
         gell_cell* dst = on_device ? cells : c->staging;
@@ -477,7 +506,49 @@ gell_status gell_cells_export(gell_ctx* c, gell_cell* cells, int capacity, int* 
         }
     }
     if (n_out) *n_out = n;
+    return cells_end(c, GELL_OK);
+}
+
+gell_status gell_cells_import_async(gell_ctx* c, const gell_cell* cells, int n) {
+    if (!c || (n > 0 && !cells) || n < 0) return GELL_ERR_INVALID_ARG;
+    if (n > c->cap) return fail(c, GELL_ERR_CAPACITY, "more cells than max_cell_num");
+    GELL_CUDA(c, cudaStreamWaitEvent(c->xfer, c->cells_ev, 0));
+    if (n > 0) {
+        GELL_CUDA(c, cudaMemcpyAsync(c->staging, cells, (size_t)n * sizeof(gell_cell), cudaMemcpyHostToDevice,
+                                     c->xfer));
+        k_import<<<blocks_for(n, 256), 256, 0, c->xfer>>>(c->staging, c->cur(), n, c->g);
+        c->launches++;
+        GELL_LAUNCH(c, "k_import");
+    }
+    GELL_CUDA(c, cudaEventRecord(c->xfer_ev, c->xfer));
+    c->xfer_pending = true;
+    c->n = n;
+    c->sorted_valid = false;
+    c->rate_valid = false;
     return GELL_OK;
+}
+
+gell_status gell_cells_export_async(gell_ctx* c, gell_cell* cells, int capacity, int* n_out) {
+    if (!c || (c->n > 0 && !cells)) return GELL_ERR_INVALID_ARG;
+    if (capacity < c->n) return fail(c, GELL_ERR_CAPACITY, "export buffer too small");
+    const int n = c->n;
+    GELL_CUDA(c, cudaStreamWaitEvent(c->xfer, c->cells_ev, 0));
+    if (n > 0) {
+        k_export<<<blocks_for(n, 256), 256, 0, c->xfer>>>(c->cur(), c->staging, n);
+        c->launches++;
+        GELL_LAUNCH(c, "k_export");
+        GELL_CUDA(c, cudaMemcpyAsync(cells, c->staging, (size_t)n * sizeof(gell_cell), cudaMemcpyDeviceToHost,
+                                     c->xfer));
+    }
+    GELL_CUDA(c, cudaEventRecord(c->xfer_ev, c->xfer));
+    c->xfer_pending = true;
+    if (n_out) *n_out = n;
+    return GELL_OK;
+}
+
+gell_status gell_wait_transfers(gell_ctx* c) {
+    if (!c) return GELL_ERR_INVALID_ARG;
+    return cells_begin(c);
 }
 
 gell_status gell_cell_count(gell_ctx* c, int* n_out) {
@@ -578,12 +649,14 @@ gell_status gell_launch_count(gell_ctx* c, int64_t* count) {
 
 gell_status gell_fm_update(gell_ctx* c) {
     if (!c) return GELL_ERR_INVALID_ARG;
-    return fm_update(c);
+    if (gell_status b = cells_begin(c)) return b;
+    return cells_end(c, fm_update(c));
 }
 
 gell_status gell_prelod(gell_ctx* c, int sub) {
     if (!c || sub < -1 || sub >= (int)c->subs.size()) return GELL_ERR_INVALID_ARG;
-    return prelod(c, sub);
+    if (gell_status b = cells_begin(c)) return b;
+    return cells_end(c, prelod(c, sub));
 }
 
 gell_status gell_lod_solver(gell_ctx* c, int sub, int substeps) {
@@ -593,24 +666,29 @@ gell_status gell_lod_solver(gell_ctx* c, int sub, int substeps) {
 
 gell_status gell_cell_birth(gell_ctx* c, int* n_out) {
     if (!c) return GELL_ERR_INVALID_ARG;
-    return birth(c, n_out);
+    if (gell_status b = cells_begin(c)) return b;
+    return cells_end(c, birth(c, n_out));
 }
 
 gell_status gell_cell_death(gell_ctx* c, int* n_out) {
     if (!c) return GELL_ERR_INVALID_ARG;
-    return death(c, n_out);
+    if (gell_status b = cells_begin(c)) return b;
+    return cells_end(c, death(c, n_out));
 }
 
 gell_status gell_mechanics_step(gell_ctx* c, int substeps) {
     if (!c || substeps < 0) return GELL_ERR_INVALID_ARG;
+    if (gell_status b = cells_begin(c)) return b;
     gell_status s = fm_update(c);
     if (s == GELL_OK) s = prelod(c, -1);
+    s = cells_end(c, s);
     if (s == GELL_OK) s = lod_solver(c, -1, substeps);
     return s;
 }
 
 gell_status gell_debug_dump(gell_ctx* c, int what, int arg, void* out, size_t bytes) {
     if (!c || !out) return GELL_ERR_INVALID_ARG;
+    if (gell_status b = cells_begin(c)) return b;
     const int n = c->n;
     switch (what) {
         case GELL_DUMP_KEYS:

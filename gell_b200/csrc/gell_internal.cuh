@@ -123,6 +123,13 @@ struct gell_ctx {
 
     gell_cell* staging = nullptr;  // cap AoS records
 
+    // queued host transfers of the cells (gell_cells_import_async / _export_async): a stream of
+    // their own, ordered after the last work that used the cells (cells_ev, recorded on `stream`),
+    // and waited for (xfer_ev) by the next work that uses them
+    cudaStream_t xfer = nullptr;
+    cudaEvent_t cells_ev = nullptr, xfer_ev = nullptr;
+    bool xfer_pending = false;
+
     // launch accounting and optional per-kernel event timing
     long long launches = 0;
     bool prof_on = false;

@@ -153,6 +153,19 @@ gell_status gell_cells_import(gell_ctx* ctx, const gell_cell* cells, int n, int 
  * count to *n_out; replaces CpuCell = GpuCell (Main.cu:151). Synchronises when on host. */
 gell_status gell_cells_export(gell_ctx* ctx, gell_cell* cells, int capacity, int* n_out,
                               int cells_on_device);
+/* Queued host transfers of the cells: gell_cells_import / gell_cells_export with host memory, but
+ * returning at once.  The copy runs on a transfer stream of the context, after the last queued work
+ * that uses the cells (fm_update, prelod, birth, death, another transfer), and the next such work
+ * waits for it; the LOD substeps do not use the cells, so a transfer queued after prelod overlaps
+ * them.  `cells` should be pinned host memory for the copy to overlap.  It must stay valid (and,
+ * for an import, unchanged) until the transfer has finished: after gell_sync, or in stream order
+ * after gell_wait_transfers.  No counterpart in the reference (its host loop copies synchronously,
+ * Main.cu:91-92,151). */
+gell_status gell_cells_import_async(gell_ctx* ctx, const gell_cell* cells, int n);
+gell_status gell_cells_export_async(gell_ctx* ctx, gell_cell* cells, int capacity, int* n_out);
+/* Make the context's stream wait (without blocking the host) for every queued transfer. */
+gell_status gell_wait_transfers(gell_ctx* ctx);
+
 /* Current cell count (the reference's host `currentnum`).  No synchronisation. */
 gell_status gell_cell_count(gell_ctx* ctx, int* n_out);
 
@@ -188,7 +201,7 @@ gell_status gell_cell_death(gell_ctx* ctx, int* n_out);
  * gell_lod_solver(-1) calls, as the reference host loop runs them (Main.cu:114-124). */
 gell_status gell_mechanics_step(gell_ctx* ctx, int substeps);
 
-/* Wait for all work queued on the context's stream. */
+/* Wait for all work queued on the context's stream and for the queued transfers. */
 gell_status gell_sync(gell_ctx* ctx);
 
 /* Debug and parity support.  Copies the named internal array to host memory `out` (room for
