@@ -116,6 +116,7 @@ def load_library() -> ctypes.CDLL:
     L.gell_cells_import_async.argtypes = [P, P, ctypes.c_int]
     L.gell_cells_export_async.argtypes = [P, P, ctypes.c_int, P]
     L.gell_wait_transfers.argtypes = [P]
+    L.gell_run_mechanics.argtypes = [P, ctypes.c_int, ctypes.c_int]
     L.gell_field_import.argtypes = [P, ctypes.c_int, P, ctypes.c_int]
     L.gell_field_export.argtypes = [P, ctypes.c_int, P, ctypes.c_int]
     L.gell_fm_update.argtypes = [P]
@@ -142,7 +143,7 @@ def load_library() -> ctypes.CDLL:
                  "gell_cell_birth", "gell_cell_death", "gell_mechanics_step", "gell_sync",
                  "gell_debug_dump", "gell_profile_enable", "gell_profile_read", "gell_launch_count",
                  "gell_selftest_division", "gell_set_option", "gell_cells_import_async",
-                 "gell_cells_export_async", "gell_wait_transfers"):
+                 "gell_cells_export_async", "gell_wait_transfers", "gell_run_mechanics"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
@@ -251,6 +252,11 @@ class Simulation:
         self._check(self.lib.gell_cells_export_async(self.h, P(_ptr(out)), len(out), ctypes.byref(cnt)),
                     "gell_cells_export_async")
         return cnt.value
+
+    def run_mechanics(self, steps: int, substeps: int = 10) -> None:
+        """`steps` mechanics steps (FM_update, PreLOD, `substeps` LOD substeps each), pairs of them
+        replayed from a captured CUDA graph; queued, no host synchronisation."""
+        self._check(self.lib.gell_run_mechanics(self.h, steps, substeps), "gell_run_mechanics")
 
     def wait_transfers(self) -> None:
         """Make the context's stream wait for every queued transfer (the host does not block)."""

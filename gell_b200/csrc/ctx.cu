@@ -186,6 +186,9 @@ static void free_all(gell_ctx* c) {
     }
     f(c->sort.hist);
     f(c->bins);
+    f(c->dev_epoch);
+    for (auto& g : c->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
     for (auto& s : c->subs) { f(s.p); f(s.rate); f(s.EF); f(s.FRS); f(s.line_flag); f(s.line_list); f(s.line_count); }
     f(c->xorwow); f(c->flags); f(c->scan_tmp); f(c->dev_count); f(c->dev_err);
     f(c->staging);
@@ -260,6 +263,7 @@ gell_status gell_create(const gell_params* params, gell_ctx** out) {
     }
     A((void**)&c->sort.hist, sort_hist_entries(c->cap) * 4);
     A((void**)&c->bins, (size_t)c->nvox * sizeof(int4));
+    A((void**)&c->dev_epoch, sizeof(int));
     A((void**)&c->flags, (cap + 1) * 4);
     A((void**)&c->scan_tmp, ((cap + 4095) / 4096 + 64) * 4 * 2);
     A((void**)&c->dev_count, 64);
@@ -272,6 +276,7 @@ gell_status gell_create(const gell_params* params, gell_ctx** out) {
         return st;
     }
     cudaMemsetAsync(c->bins, 0, (size_t)c->nvox * sizeof(int4), c->stream);
+    if (c->dev_epoch) cudaMemsetAsync(c->dev_epoch, 0, sizeof(int), c->stream);
     cudaMemsetAsync(c->dev_err, 0, 64, c->stream);
     if (P.rng_mode == GELL_RNG_XORWOW) {
         st = init_xorwow(c);
@@ -683,7 +688,95 @@ gell_status gell_mechanics_step(gell_ctx* c, int substeps) {
     if (s == GELL_OK) s = prelod(c, -1);
     s = cells_end(c, s);
     if (s == GELL_OK) s = lod_solver(c, -1, substeps);
+    if (s == GELL_OK) c->stepped = true;
     return s;
+}
+
+}  // extern "C"
+
+// Which buffer of each double-buffered cell field is current: a captured graph is only valid for
+// the assignment it was captured with.
+static uint32_t buffer_parity(const gell_ctx* c) {
+    return (uint32_t)(c->sign.c | c->mesh.c << 1 | c->posr.c << 2 | c->force.c << 3 | c->oldf.c << 4 |
+                      c->V.c << 5 | c->Vf.c << 6 | c->Vcs.c << 7 | c->Vns.c << 8 | c->clock.c << 9 |
+                      c->phase.c << 10);
+}
+
+static gell_status one_mechanics_step(gell_ctx* c, int substeps) {
+    gell_status s = fm_update(c);
+    if (s == GELL_OK) s = prelod(c, -1);
+    if (s == GELL_OK) s = lod_solver(c, -1, substeps);
+    return s;
+}
+
+// Capture two mechanics steps on the context's stream into cache entry `gs`.
+static gell_status capture_step_graph(gell_ctx* c, gell_ctx::StepGraph& gs, int substeps) {
+    if (gs.exec) {
+        cudaGraphExecDestroy(gs.exec);
+        gs.exec = nullptr;
+    }
+    const uint32_t parity = buffer_parity(c);
+    const long long l0 = c->launches;
+    GELL_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    gell_status st = one_mechanics_step(c, substeps);
+    if (st == GELL_OK) st = one_mechanics_step(c, substeps);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    // nothing ran during the capture: the launches are counted when the graph is replayed
+    gs.launches = c->launches - l0;
+    c->launches = l0;
+    if (st != GELL_OK) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
+    const cudaError_t ei = cudaGraphInstantiate(&gs.exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+        gs.exec = nullptr;
+        return cuda_fail(c, ei, "cudaGraphInstantiate");
+    }
+    gs.n = c->n;
+    gs.substeps = substeps;
+    gs.nsub = (int)c->subs.size();
+    gs.parity = parity;
+    return GELL_OK;
+}
+
+extern "C" {
+
+gell_status gell_run_mechanics(gell_ctx* c, int steps, int substeps) {
+    if (!c || steps < 0 || substeps < 0) return GELL_ERR_INVALID_ARG;
+    if (steps == 0) return GELL_OK;
+    if (gell_status b = cells_begin(c)) return b;
+    int left = steps;
+    gell_status st = GELL_OK;
+    if (!c->stepped) {
+        // the first step of a context runs outside any capture (first-use set-up of the kernels)
+        st = one_mechanics_step(c, substeps);
+        --left;
+        c->stepped = st == GELL_OK;
+    }
+    if (st == GELL_OK && left >= 2 && !c->prof_on && c->n > 0) {
+        const uint32_t par = buffer_parity(c);
+        gell_ctx::StepGraph* gs = nullptr;
+        for (auto& e : c->graphs)
+            if (e.exec && e.n == c->n && e.substeps == substeps && e.nsub == (int)c->subs.size() && e.parity == par)
+                gs = &e;
+        if (!gs) {
+            gs = c->graphs[0].used <= c->graphs[1].used ? &c->graphs[0] : &c->graphs[1];
+            st = capture_step_graph(c, *gs, substeps);
+        }
+        gs->used = ++c->graph_clock;
+        for (; left >= 2 && st == GELL_OK && gs->exec; left -= 2) {
+            const cudaError_t e = cudaGraphLaunch(gs->exec, c->stream);
+            if (e != cudaSuccess) st = cuda_fail(c, e, "cudaGraphLaunch");
+            c->launches += gs->launches;
+        }
+    }
+    for (; left > 0 && st == GELL_OK; --left) st = one_mechanics_step(c, substeps);
+    if (st == GELL_OK) c->stepped = true;
+    return cells_end(c, st);
 }
 
 gell_status gell_debug_dump(gell_ctx* c, int what, int arg, void* out, size_t bytes) {

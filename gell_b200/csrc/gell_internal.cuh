@@ -106,12 +106,25 @@ struct gell_ctx {
 
     gell::SortScratch sort;
     int4* bins = nullptr;
-    int epoch = 0;
+    int* dev_epoch = nullptr;  // cell-list epoch (device: replayed graphs read the current one)
     bool sorted_valid = false;  // keys/perm describe the current order
 
     std::vector<gell::Substrate> subs;
     bool rate_valid = false;
     bool exact_chain = false;  // GELL_OPT_EXACT_CHAIN
+
+    // gell_run_mechanics: captured graphs of two mechanics steps and what each was captured for
+    // (two entries: an odd number of steps flips the double buffers to the other assignment)
+    struct StepGraph {
+        cudaGraphExec_t exec = nullptr;
+        int n = -1, substeps = -1, nsub = -1;
+        uint32_t parity = 0;
+        long long launches = 0;  // kernels in one replay
+        long long used = 0;
+    };
+    StepGraph graphs[2];
+    long long graph_clock = 0;
+    bool stepped = false;  // a mechanics step has run outside a capture (kernel set-up done)
 
     // PD
     curandState* xorwow = nullptr;

@@ -15,8 +15,11 @@ namespace gell {
 
 namespace {
 
-__global__ void k_keys(CellsSoA c, int n, Geom g, uint32_t* __restrict__ keys) {
+// Also advances the cell-list epoch, which lives in device memory so that a captured step reads
+// the current one when it is replayed.
+__global__ void k_keys(CellsSoA c, int n, Geom g, uint32_t* __restrict__ keys, int* __restrict__ epoch) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) *epoch += 1;
     if (i >= n) return;
     const float4 pr = c.posr[i];
     const int3 b = find_bin(pr.x, pr.y, pr.z, g.len);
@@ -30,9 +33,11 @@ __global__ void k_keys(CellsSoA c, int n, Geom g, uint32_t* __restrict__ keys) {
 }
 
 __global__ void k_gather(CellsSoA s, CellsSoA d, const uint32_t* __restrict__ keys,
-                         const uint32_t* __restrict__ perm, int n, int4* __restrict__ bins, int epoch) {
+                         const uint32_t* __restrict__ perm, int n, int4* __restrict__ bins,
+                         const int* __restrict__ epoch_p) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const int epoch = *epoch_p;
     const int j = (int)perm[i];
     d.sign[i] = s.sign[j];
     const int m = s.mesh[j];
@@ -59,7 +64,7 @@ __global__ void k_gather(CellsSoA s, CellsSoA d, const uint32_t* __restrict__ ke
 struct MechArgs {
     CellsSoA cur, alt;
     const int4* bins;
-    int epoch;
+    const int* epoch;
     int n;
     Geom g;
     float max_dist, cccr, ccca;
@@ -90,6 +95,7 @@ __global__ void __launch_bounds__(256) k_force_move(MechArgs a) {
     }
     const int N = a.g.N;
     const long long NN = (long long)N * N;
+    const int epoch = *a.epoch;
     const int3 b = find_bin(pr.x, pr.y, pr.z, a.g.len);
     float fx = 0.f, fy = 0.f, fz = 0.f;
     float thres = a.max_dist;
@@ -102,7 +108,7 @@ __global__ void __launch_bounds__(256) k_force_move(MechArgs a) {
         const int xi = b.x - 1 + o / 9, yi = b.y - 1 + (o / 3) % 3, zi = b.z - 1 + o % 3;
         if (!inside(xi, yi, zi, N)) continue;
         const int4 e = a.bins[xi + (long long)yi * N + zi * NN];
-        if (e.z != a.epoch) continue;
+        if (e.z != epoch) continue;
 #pragma unroll 1
         for (int j = e.x; j <= e.y; ++j) {
             if (!a.cur.sign[j]) continue;
@@ -188,20 +194,20 @@ static int key_bits(int N) {
 
 gell_status fm_update(gell_ctx* c) {
     const int n = c->n;
-    c->epoch += 1;
     if (n > 0) {
-        GELL_KERNEL(c, "k_keys", k_keys<<<blocks_for(n, 256), 256, 0, c->stream>>>(c->cur(), n, c->g, c->sort.keys[0]));
+        GELL_KERNEL(c, "k_keys", k_keys<<<blocks_for(n, 256), 256, 0, c->stream>>>(c->cur(), n, c->g, c->sort.keys[0],
+                                                                                c->dev_epoch));
         gell_status st = radix_sort(c, n, key_bits(c->g.N), true);
         if (st != GELL_OK) return st;
         const int w = c->sort.which;
         GELL_KERNEL(c, "k_gather", k_gather<<<blocks_for(n, 256), 256, 0, c->stream>>>(c->cur(), c->alt(), c->sort.keys[w], c->sort.vals[w], n,
-                                                              c->bins, c->epoch));
+                                                              c->bins, c->dev_epoch));
         c->swap_all();
         MechArgs a;
         a.cur = c->cur();
         a.alt = c->alt();
         a.bins = c->bins;
-        a.epoch = c->epoch;
+        a.epoch = c->dev_epoch;
         a.n = n;
         a.g = c->g;
         a.max_dist = c->P.cc_max_dist;

@@ -201,6 +201,14 @@ gell_status gell_cell_death(gell_ctx* ctx, int* n_out);
  * gell_lod_solver(-1) calls, as the reference host loop runs them (Main.cu:114-124). */
 gell_status gell_mechanics_step(gell_ctx* ctx, int substeps);
 
+/* `steps` mechanics steps, each gell_fm_update, gell_prelod(-1) and `substeps` gell_lod_solver(-1)
+ * calls: the reference host loop between two biology steps (Main.cu:114-124), with an integer step
+ * count.  Pairs of steps are replayed from a CUDA graph captured on the context's stream (two steps
+ * bring every double buffer back to where it was); the graph is captured again when the cell count,
+ * the substrates, `substeps` or the buffer assignment have changed, and not used while per-kernel
+ * profiling is on.  Queued on the context's stream, no host synchronisation. */
+gell_status gell_run_mechanics(gell_ctx* ctx, int steps, int substeps);
+
 /* Wait for all work queued on the context's stream and for the queued transfers. */
 gell_status gell_sync(gell_ctx* ctx);
 
