@@ -121,6 +121,12 @@ private:
     int index_ = -1;
 };
 
+// `steps` mechanics steps of FM_update, PreLOD and `substeps` LOD substeps (Main.cu:114-124 with an
+// integer count), pairs of them replayed from a captured CUDA graph.
+inline void run_mechanics(Context& c, int steps, int substeps = 10) {
+    check(gell_run_mechanics(c.get(), steps, substeps), c.get(), "run_mechanics");
+}
+
 // CellBirth_kernel / CellDeath_kernel (include/PDkernel.cuh:88-117): return the new count.
 inline int CellBirth_kernel(Context& c) {
     int n = 0;
@@ -130,6 +136,19 @@ inline int CellBirth_kernel(Context& c) {
 inline int CellDeath_kernel(Context& c) {
     int n = 0;
     check(gell_cell_death(c.get(), &n), c.get(), "CellDeath_kernel");
+    return n;
+}
+
+// The reference's time loop (Main.cu:108-128) with integer counts: every biology step runs
+// `mech_per_bio` mechanics steps (each with `substeps` LOD substeps of every substrate), then birth
+// and death.  Returns the final cell count.
+inline int run(Context& c, int bio_steps, int mech_per_bio = 60, int substeps = 10) {
+    int n = c.count();
+    for (int b = 0; b < bio_steps; ++b) {
+        run_mechanics(c, mech_per_bio, substeps);
+        CellBirth_kernel(c);
+        n = CellDeath_kernel(c);
+    }
     return n;
 }
 

@@ -127,6 +127,8 @@ int main() {
         o2.LODsolver();
         int n = gell::CellBirth_kernel(ctx);
         n = gell::CellDeath_kernel(ctx);
+        gell::run_mechanics(ctx, 4, 10);
+        n = gell::run(ctx, 1, 60, 10);
         std::printf("ran %d\n", n);
         return 0;
     } catch (const gell::Error& e) {
