@@ -308,6 +308,100 @@ def run_gell(args, rank, world, local_rank):
     return line
 
 
+# ---------------------------------------------------------------------------- birth/death workload
+
+C3_N, C3_CELLS, C3_CAP, C3_BIO = 600, 5_000_000, 10_000_000, 60
+C3_WORKLOAD = ("plain method with stochastic birth/death: 600^3 voxels at 10 um, oxygen + drug (FP32), "
+               "5*10^6 cells, Philox draws; every 60 mechanics steps (one 6-min biology step) birth "
+               "before and death after, as the reference loop runs them")
+
+
+def run_c3(args, rank, world, local_rank):
+    """--workload c3: K mechanics steps in biology periods of 60 (birth, 60 steps, death)."""
+    import torch
+    import gell_b200 as gb
+
+    torch.cuda.set_device(local_rank)
+    length = LENGTH
+    cells = gb.lattice_spheroid(C3_CELLS, C3_N * length / 2, 3, length, C3_N)
+    gb.seed_ki67_states(cells, 11)
+    sim = gb.Simulation(voxel_num=C3_N, voxel_length=length, max_cell_num=C3_CAP, rng_mode=gb.GELL_RNG_PHILOX,
+                        seed=20260101)
+    sim.add_substrate(gb.oxygen())
+    sim.add_substrate(gb.drug())
+    stream = torch.cuda.Stream()
+    sim.set_stream(stream)
+    sim.import_cells(cells)
+    sim.run_mechanics(args.warmup, SUBSTEPS)
+    sim.sync()
+    n0 = sim.count()
+
+    props = torch.cuda.get_device_properties(local_rank)
+    uuid = getattr(props, "uuid", None)
+    uuid = f"GPU-{uuid}" if uuid is not None and not str(uuid).startswith("GPU-") else uuid
+    sampler = ClockSampler(str(uuid) if uuid else None)
+    sampler.start()
+    time.sleep(0.3)
+    K = args.steps
+    ev = []
+    cell_steps = 0
+    births = deaths = 0
+    t_bio = 0.0
+    if world > 1:
+        import torch.distributed as td
+        td.barrier()
+    torch.cuda.synchronize()
+    e_start = torch.cuda.Event(enable_timing=True)
+    e_start.record(stream)
+    done = 0
+    while done < K:
+        m = min(C3_BIO, K - done)
+        a, b, c2, d = (torch.cuda.Event(enable_timing=True) for _ in range(4))
+        a.record(stream)
+        nb = sim.CellBirth_kernel()
+        b.record(stream)
+        sim.run_mechanics(m, SUBSTEPS)
+        c2.record(stream)
+        nd = sim.CellDeath_kernel()
+        d.record(stream)
+        ev.append((a, b, c2, d))
+        births += nb - (n0 if done == 0 else last)
+        deaths += nb - nd
+        cell_steps += nb * m
+        last = nd
+        done += m
+    e_end = torch.cuda.Event(enable_timing=True)
+    e_end.record(stream)
+    torch.cuda.synchronize()
+    sampler.stop()
+    t_all = e_start.elapsed_time(e_end)
+    for a, b, c2, d in ev:
+        t_bio += a.elapsed_time(b) + c2.elapsed_time(d)
+    times = np.array([t_all, t_bio], np.float64)
+    cnt = np.array([cell_steps], np.float64)
+    if world > 1:
+        times, cnt = reduce_over_ranks(times, cnt, "cuda")
+    t_all, t_bio = times
+    line = None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": cnt[0] / (t_all / 1e3), "unit": "cell-updates/s", "n_gpus": world,
+            "steps": K, "warmup": args.warmup, "ms_per_step": t_all / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: seeded jittered-lattice spheroid of 5*10^6 cells (radius ~1 mm) with seeded Ki-67 "
+                    "phases and clocks, fields start at the boundary values",
+            "config": {"workload": C3_WORKLOAD, "voxels": C3_N ** 3, "substrates": 2, "cells": C3_CELLS,
+                       "substeps_per_step": SUBSTEPS, "voxel_um": length, "biology_period_steps": C3_BIO,
+                       "l2": "inputs larger than L2: each field is 864 MB", "parallelism": "replicas",
+                       "cells_per_step": "array slots after the period's birth (cells dead since then included)"},
+            "components": {"ms_birth_plus_death_per_period": t_bio / max(len(ev), 1),
+                           "births": int(births), "removed": int(deaths), "cells_end": int(last)},
+            "gpu_launches": None, "clocks": sampler.summary(),
+        }
+    sim.close()
+    return line
+
+
 # ---------------------------------------------------------------------------- CPU (oracle) leg
 
 class CpuWork:
@@ -395,6 +489,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("gell", "reference"), default="gell")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=("large", "c3"), default="large",
+                    help="large: 400^3, 10^6 cells (the headline line); c3: 600^3, 5*10^6 cells with birth/death")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -414,6 +510,14 @@ def main():
         import torch.distributed as td
         torch.cuda.set_device(local_rank)
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    if args.workload == "c3":
+        line = run_c3(args, rank, world, local_rank)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            import torch.distributed as td
+            td.destroy_process_group()
+        return
     line = run_gell(args, rank, world, local_rank)
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:

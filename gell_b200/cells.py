@@ -107,3 +107,24 @@ def lattice_spheroid(n: int, center: float, seed: int, voxel_length: float, voxe
     pts += rng.uniform(-0.1 * a, 0.1 * a, size=pts.shape)
     pts += center
     return live_cells(pts, _radii(rng, n), voxel_length, voxel_num)
+
+
+def seed_ki67_states(c: np.ndarray, seed: int) -> np.ndarray:
+    """Spread cells over the Ki-67 phases so that a run of a few biology steps divides and
+    removes cells (a population that starts all quiescent has almost no events for hundreds of
+    minutes: the premitotic phase lasts 780 min).  Seeded draws (Philox): 60% quiescent, 15%
+    premitotic with clocks U[0, 780), 10% postmitotic with clocks U[0, 150), 5% each apoptotic,
+    early necrotic and late necrotic; a third of the dead cells have cytoplasm already below the
+    removal threshold (Vcs 20 um^3)."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    n = len(c)
+    ph = rng.choice(np.array([0, 1, 2, 3, 4, 5], np.int32), n, p=[0.60, 0.15, 0.10, 0.05, 0.05, 0.05])
+    clock = np.zeros(n, np.float32)
+    clock[ph == 1] = rng.uniform(0.0, 780.0, int((ph == 1).sum())).astype(np.float32)
+    clock[ph == 2] = rng.uniform(0.0, 150.0, int((ph == 2).sum())).astype(np.float32)
+    c["phase"] = ph
+    c["cell_clock"] = clock
+    dead = np.flatnonzero(ph >= 3)
+    low = dead[rng.random(len(dead)) < 1.0 / 3.0]
+    c["Vcs"][low] = np.float32(20.0)
+    return c

@@ -139,14 +139,14 @@ inline int CellDeath_kernel(Context& c) {
     return n;
 }
 
-// The reference's time loop (Main.cu:108-128) with integer counts: every biology step runs
-// `mech_per_bio` mechanics steps (each with `substeps` LOD substeps of every substrate), then birth
-// and death.  Returns the final cell count.
+// The reference's time loop (Main.cu:108-128) with integer counts: every biology step is birth,
+// then `mech_per_bio` mechanics steps (each with `substeps` LOD substeps of every substrate), then
+// death.  Returns the final cell count.
 inline int run(Context& c, int bio_steps, int mech_per_bio = 60, int substeps = 10) {
     int n = c.count();
     for (int b = 0; b < bio_steps; ++b) {
-        run_mechanics(c, mech_per_bio, substeps);
         CellBirth_kernel(c);
+        run_mechanics(c, mech_per_bio, substeps);
         n = CellDeath_kernel(c);
     }
     return n;
