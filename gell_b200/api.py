@@ -117,6 +117,13 @@ def load_library() -> ctypes.CDLL:
     L.gell_cells_export_async.argtypes = [P, P, ctypes.c_int, P]
     L.gell_wait_transfers.argtypes = [P]
     L.gell_run_mechanics.argtypes = [P, ctypes.c_int, ctypes.c_int]
+    L.gell_write_cells_csv.argtypes = [P, ctypes.c_int, ctypes.c_char_p]
+    L.gell_save_cells_csv.argtypes = [P, ctypes.c_char_p]
+    L.gell_save_field_csv.argtypes = [P, ctypes.c_int, ctypes.c_char_p]
+    L.gell_save_field_slice_csv.argtypes = [P, ctypes.c_int, ctypes.c_char_p]
+    L.gell_checkpoint_save.argtypes = [P, ctypes.c_char_p]
+    L.gell_checkpoint_load.argtypes = [P, ctypes.c_char_p]
+    L.gell_reference_spheroid.argtypes = [P, ctypes.c_int, ctypes.c_float, ctypes.c_uint32, P]
     L.gell_field_import.argtypes = [P, ctypes.c_int, P, ctypes.c_int]
     L.gell_field_export.argtypes = [P, ctypes.c_int, P, ctypes.c_int]
     L.gell_fm_update.argtypes = [P]
@@ -143,7 +150,10 @@ def load_library() -> ctypes.CDLL:
                  "gell_cell_birth", "gell_cell_death", "gell_mechanics_step", "gell_sync",
                  "gell_debug_dump", "gell_profile_enable", "gell_profile_read", "gell_launch_count",
                  "gell_selftest_division", "gell_set_option", "gell_cells_import_async",
-                 "gell_cells_export_async", "gell_wait_transfers", "gell_run_mechanics"):
+                 "gell_cells_export_async", "gell_wait_transfers", "gell_run_mechanics",
+                 "gell_write_cells_csv", "gell_save_cells_csv", "gell_save_field_csv",
+                 "gell_save_field_slice_csv", "gell_checkpoint_save", "gell_checkpoint_load",
+                 "gell_reference_spheroid"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
@@ -258,6 +268,22 @@ class Simulation:
         replayed from a captured CUDA graph; queued, no host synchronisation."""
         self._check(self.lib.gell_run_mechanics(self.h, steps, substeps), "gell_run_mechanics")
 
+    # -- snapshots and checkpoints
+    def save_cells_csv(self, path: str) -> None:
+        self._check(self.lib.gell_save_cells_csv(self.h, os.fsencode(path)), "gell_save_cells_csv")
+
+    def save_field_csv(self, sub: int, path: str) -> None:
+        self._check(self.lib.gell_save_field_csv(self.h, sub, os.fsencode(path)), "gell_save_field_csv")
+
+    def save_field_slice_csv(self, sub: int, path: str) -> None:
+        self._check(self.lib.gell_save_field_slice_csv(self.h, sub, os.fsencode(path)), "gell_save_field_slice_csv")
+
+    def checkpoint_save(self, path: str) -> None:
+        self._check(self.lib.gell_checkpoint_save(self.h, os.fsencode(path)), "gell_checkpoint_save")
+
+    def checkpoint_load(self, path: str) -> None:
+        self._check(self.lib.gell_checkpoint_load(self.h, os.fsencode(path)), "gell_checkpoint_load")
+
     def wait_transfers(self) -> None:
         """Make the context's stream wait for every queued transfer (the host does not block)."""
         self._check(self.lib.gell_wait_transfers(self.h), "gell_wait_transfers")
@@ -360,3 +386,23 @@ class Simulation:
     def dump_ef(self, sub: int) -> tuple[np.ndarray, np.ndarray]:
         ef = self._dump(GELL_DUMP_EF, sub, np.float32, 2 * self.N)
         return ef[:self.N], ef[self.N:]
+
+
+def write_cells_csv(cells: np.ndarray, path: str) -> None:
+    """The reference's savecsv_cell format for host records (no GPU needed)."""
+    if cells.dtype != CELL_DTYPE:
+        raise TypeError("cells must have gell_b200.CELL_DTYPE")
+    c = np.ascontiguousarray(cells)
+    st = load_library().gell_write_cells_csv(P(c.ctypes.data if len(c) else 0), len(c), os.fsencode(path))
+    if st != GELL_OK:
+        raise GellError(st, "gell_write_cells_csv")
+
+
+def reference_spheroid(n: int, cell_radius: float = 8.4, seed: int = 1, **param_overrides) -> np.ndarray:
+    """The reference's initial tumour (Cell_sphere_Initialization) for the given parameters."""
+    p = default_params(**param_overrides)
+    out = np.zeros(max(n, 1), CELL_DTYPE)
+    st = load_library().gell_reference_spheroid(ctypes.byref(p), n, cell_radius, seed, P(out.ctypes.data))
+    if st != GELL_OK:
+        raise GellError(st, "gell_reference_spheroid")
+    return out[:n]

@@ -270,6 +270,40 @@ gell_status gell_sort_keys_noalloc(const int32_t* keys, int32_t* sorted_keys, in
 enum { GELL_OPT_EXACT_CHAIN = 1 };
 gell_status gell_set_option(gell_ctx* ctx, int option, int64_t value);
 
+/*
+ * Snapshots in the reference's CSV formats, printed with its own format strings so that equal data
+ * gives identical files.  gell_write_cells_csv: `n` records from host memory as savecsv_cell
+ * (include/FileSave.cuh:24-33): Index,Sign,Phase,x,y,z,r,V,Vns,Vcs.  gell_save_cells_csv: the
+ * context's current cells, the same way.  gell_save_field_csv: substrate `substrate` as savecsv_mesh
+ * (include/FileSave.cuh:35-49), one i,j,k,Concentration row per voxel, x fastest.
+ * gell_save_field_slice_csv: the plane z = N/2 as savecsv_meshslice writes the slice GPU_Get_Slice
+ * takes (include/FileSave.cuh:50-64, include/LODkernel.cuh:174-181).  These synchronise.
+ */
+gell_status gell_write_cells_csv(const gell_cell* cells, int n, const char* path);
+gell_status gell_save_cells_csv(gell_ctx* ctx, const char* path);
+gell_status gell_save_field_csv(gell_ctx* ctx, int substrate, const char* path);
+gell_status gell_save_field_slice_csv(gell_ctx* ctx, int substrate, const char* path);
+
+/*
+ * Checkpoint and resume (no counterpart in the reference, which writes CSV snapshots only).
+ * gell_checkpoint_save writes the state between two calls: parameters, substrates, cells, fields,
+ * the cell-list epoch, the biology step counter and, with XORWOW draws, every slot's generator
+ * state.  gell_checkpoint_load restores it into a context created with the same parameters and
+ * substrates (GELL_ERR_STATE otherwise); the run then continues exactly as it would have without
+ * the interruption.  Both synchronise.
+ */
+gell_status gell_checkpoint_save(gell_ctx* ctx, const char* path);
+gell_status gell_checkpoint_load(gell_ctx* ctx, const char* path);
+
+/*
+ * The reference's initial tumour (Cell_sphere_Initialization, include/Initialization.cuh:15-43):
+ * n quiescent cells of radius `cell_radius` (Tumor_Cell_Radius, 8.4 um) drawn uniformly in a ball
+ * of radius cell_radius * n^(1/3) / 1.612 * 1.87 at the centre of the grid, with the reference's
+ * default volumes.  Positions come from the C library's rand() sequence for `seed` (the reference
+ * never seeds it, which is seed 1), computed by a private copy of that generator.  Host only.
+ */
+gell_status gell_reference_spheroid(const gell_params* p, int n, float cell_radius, uint32_t seed, gell_cell* out);
+
 /* Number of kernels this context has launched (always counted). */
 gell_status gell_launch_count(gell_ctx* ctx, int64_t* count);
 

@@ -39,6 +39,8 @@
 #include "FMkernel.cuh"
 #include "LODkernel.cuh"
 #include "PDkernel.cuh"
+#include "FileSave.cuh"
+#include "Initialization.cuh"
 
 #include <cstdio>
 #include <cstring>
@@ -80,6 +82,20 @@ float gref_o2_consume(const Cell* c) { Cell t = *c; return t.O2_consume(); }
 void gref_volume_update(Cell* c) { c->Volume_update(); }
 int gref_phase_update(Cell* c, float rnd, float o2) { return c->Phase_update_ki67adv(rnd, o2) ? 1 : 0; }
 void gref_radius_update(Cell* c) { c->Radius_update(); }
+
+// ---- the reference's snapshot writers and initial spheroid (host code)
+int gref_savecsv_cell(const Cell* cells, int n, const char* path) {
+    thrust::host_vector<Cell> h(cells, cells + n);
+    savecsv_cell(h, n, std::string(path));
+    return 0;
+}
+int gref_init_sphere(unsigned seed, int n, Cell* out) {
+    srand(seed);
+    thrust::host_vector<Cell> h(n);
+    Cell_sphere_Initialization(h, n);
+    for (int i = 0; i < n; ++i) out[i] = h[i];
+    return 0;
+}
 
 // ---- the same Cell member function compiled for and run on the GPU
 static __global__ void gref_k_volume(Cell* c, int n) {
@@ -231,6 +247,19 @@ static float time_it(int warm, int iters, void (*f)(GRef*), GRef* g) {
 static void f_fm(GRef* g) { g->mech->FM_update(*g->cells, g->n); }
 static void f_prelod(GRef* g) { g->mesh->PreLOD(thrust::raw_pointer_cast(g->cells->data()), g->n); }
 static void f_lod(GRef* g) { g->mesh->LODsolver(thrust::raw_pointer_cast(g->cells->data()), g->n); }
+// savecsv_mesh / savecsv_meshslice of the mesh's current field (include/FileSave.cuh:35-64)
+int gref_savecsv_mesh(void* h, const char* path) {
+    GRef* g = (GRef*)h;
+    g->mesh->move_to_CPU();
+    savecsv_mesh(g->mesh, std::string(path));
+    return (int)cudaGetLastError();
+}
+int gref_savecsv_meshslice(void* h, const char* path) {
+    GRef* g = (GRef*)h;
+    g->mesh->Slice_to_CPU();
+    savecsv_meshslice(g->mesh, std::string(path));
+    return (int)cudaGetLastError();
+}
 float gref_time_fm(void* h, int warm, int iters) { return time_it(warm, iters, f_fm, (GRef*)h); }
 float gref_time_prelod(void* h, int warm, int iters) { return time_it(warm, iters, f_prelod, (GRef*)h); }
 float gref_time_lod(void* h, int warm, int iters) { return time_it(warm, iters, f_lod, (GRef*)h); }

@@ -43,6 +43,10 @@ def lib(name: str) -> ctypes.CDLL:
         for f in ("gref_get_field", "gref_set_field", "gref_get_rate", "gref_set_rate"):
             getattr(L, f).argtypes = [P, P]
         L.gref_get_ef.argtypes = [P, P, P]
+        L.gref_savecsv_cell.argtypes = [P, ctypes.c_int, ctypes.c_char_p]
+        L.gref_init_sphere.argtypes = [ctypes.c_uint, ctypes.c_int, P]
+        L.gref_savecsv_mesh.argtypes = [P, ctypes.c_char_p]
+        L.gref_savecsv_meshslice.argtypes = [P, ctypes.c_char_p]
         L.gref_volume_update_device.argtypes = [P, ctypes.c_int]
         L.gref_volume_update_device.restype = ctypes.c_int
         for f in ("gref_time_fm", "gref_time_prelod", "gref_time_lod"):
@@ -140,6 +144,12 @@ class RefSim:
 
     def death(self) -> int:
         return self.L.gref_death(self.h)
+
+    def savecsv_mesh(self, path):
+        assert self.L.gref_savecsv_mesh(self.h, os.fsencode(path)) == 0
+
+    def savecsv_meshslice(self, path):
+        assert self.L.gref_savecsv_meshslice(self.h, os.fsencode(path)) == 0
 
     def time_fm(self, warm, iters):
         return self.L.gref_time_fm(self.h, warm, iters)
