@@ -124,6 +124,12 @@ def load_library() -> ctypes.CDLL:
     L.gell_checkpoint_save.argtypes = [P, ctypes.c_char_p]
     L.gell_checkpoint_load.argtypes = [P, ctypes.c_char_p]
     L.gell_reference_spheroid.argtypes = [P, ctypes.c_int, ctypes.c_float, ctypes.c_uint32, P]
+    L.gell_ensemble_create.argtypes = [P, ctypes.c_int, P]
+    L.gell_ensemble_destroy.argtypes = [P]
+    L.gell_ensemble_configure.argtypes = [P, ctypes.c_int, ctypes.c_int]
+    L.gell_ensemble_run_mechanics.argtypes = [P, ctypes.c_int, ctypes.c_int]
+    L.gell_ensemble_tune.argtypes = [P, ctypes.c_int, P, P, P]
+    L.gell_ensemble_sync.argtypes = [P]
     L.gell_field_import.argtypes = [P, ctypes.c_int, P, ctypes.c_int]
     L.gell_field_export.argtypes = [P, ctypes.c_int, P, ctypes.c_int]
     L.gell_fm_update.argtypes = [P]
@@ -153,7 +159,9 @@ def load_library() -> ctypes.CDLL:
                  "gell_cells_export_async", "gell_wait_transfers", "gell_run_mechanics",
                  "gell_write_cells_csv", "gell_save_cells_csv", "gell_save_field_csv",
                  "gell_save_field_slice_csv", "gell_checkpoint_save", "gell_checkpoint_load",
-                 "gell_reference_spheroid"):
+                 "gell_reference_spheroid", "gell_ensemble_create", "gell_ensemble_destroy",
+                 "gell_ensemble_configure", "gell_ensemble_run_mechanics", "gell_ensemble_tune",
+                 "gell_ensemble_sync"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
@@ -406,3 +414,55 @@ def reference_spheroid(n: int, cell_radius: float = 8.4, seed: int = 1, **param_
     if st != GELL_OK:
         raise GellError(st, "gell_reference_spheroid")
     return out[:n]
+
+
+class Ensemble:
+    """Independent simulations stepped together (gell_ensemble_*): pairs of mechanics steps of all
+    members replay one CUDA graph whose parallel branches run the members side by side."""
+
+    def __init__(self, members: list[Simulation]):
+        self.lib = load_library()
+        self.members = list(members)
+        arr = (P * len(members))(*[m.h for m in members])
+        h = P()
+        st = self.lib.gell_ensemble_create(arr, len(members), ctypes.byref(h))
+        if st != GELL_OK:
+            raise GellError(st, "gell_ensemble_create")
+        self.h = h
+
+    def _check(self, st: int, what: str) -> None:
+        if st != GELL_OK:
+            raise GellError(st, what)
+
+    def configure(self, branches: int, sweep_warps: int = 0) -> None:
+        self._check(self.lib.gell_ensemble_configure(self.h, branches, sweep_warps), "gell_ensemble_configure")
+
+    def run_mechanics(self, steps: int, substeps: int = 10) -> None:
+        self._check(self.lib.gell_ensemble_run_mechanics(self.h, steps, substeps), "gell_ensemble_run_mechanics")
+
+    def tune(self, substeps: int = 10) -> tuple[int, int, int]:
+        """Returns (steps taken by every member, best branch count, best sweep tile width)."""
+        t, b, w = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.gell_ensemble_tune(self.h, substeps, ctypes.byref(t), ctypes.byref(b), ctypes.byref(w)),
+                    "gell_ensemble_tune")
+        return t.value, b.value, w.value
+
+    def sync(self) -> None:
+        self._check(self.lib.gell_ensemble_sync(self.h), "gell_ensemble_sync")
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.gell_ensemble_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -465,15 +465,17 @@ gell_status gell_substrate_add(gell_ctx* c, const gell_substrate* s, int* index_
 
 // Work on `stream` that uses the cells first waits for the queued transfers, and afterwards marks
 // the point the next queued transfer has to wait for.
-static gell_status cells_begin(gell_ctx* c) {
+namespace gell {
+gell_status cells_begin(gell_ctx* c) {
     if (c->xfer_pending) GELL_CUDA(c, cudaStreamWaitEvent(c->stream, c->xfer_ev, 0));
     return GELL_OK;
 }
-static gell_status cells_end(gell_ctx* c, gell_status st) {
+gell_status cells_end(gell_ctx* c, gell_status st) {
     if (st != GELL_OK) return st;
     GELL_CUDA(c, cudaEventRecord(c->cells_ev, c->stream));
     return GELL_OK;
 }
+}  // namespace gell
 
 extern "C" {
 
@@ -642,6 +644,10 @@ gell_status gell_set_option(gell_ctx* c, int option, int64_t value) {
     if (!c) return GELL_ERR_INVALID_ARG;
     switch (option) {
         case GELL_OPT_EXACT_CHAIN: c->exact_chain = value != 0; return GELL_OK;
+        case GELL_OPT_SWEEP_WARPS:
+            if (value < 0 || value > 4) return fail(c, GELL_ERR_INVALID_ARG, "sweep warps outside 0..4");
+            c->sweep_warps = (int)value;
+            return GELL_OK;
         default: return fail(c, GELL_ERR_INVALID_ARG, "unknown option");
     }
 }
@@ -696,13 +702,14 @@ gell_status gell_mechanics_step(gell_ctx* c, int substeps) {
 
 // Which buffer of each double-buffered cell field is current: a captured graph is only valid for
 // the assignment it was captured with.
-static uint32_t buffer_parity(const gell_ctx* c) {
+namespace gell {
+uint32_t buffer_parity(const gell_ctx* c) {
     return (uint32_t)(c->sign.c | c->mesh.c << 1 | c->posr.c << 2 | c->force.c << 3 | c->oldf.c << 4 |
                       c->V.c << 5 | c->Vf.c << 6 | c->Vcs.c << 7 | c->Vns.c << 8 | c->clock.c << 9 |
                       c->phase.c << 10);
 }
 
-static gell_status one_mechanics_step(gell_ctx* c, int substeps) {
+gell_status one_mechanics_step(gell_ctx* c, int substeps) {
     gell_status s = fm_update(c);
     if (s == GELL_OK) s = prelod(c, -1);
     if (s == GELL_OK) s = lod_solver(c, -1, substeps);
@@ -710,6 +717,8 @@ static gell_status one_mechanics_step(gell_ctx* c, int substeps) {
 }
 
 // Capture two mechanics steps on the context's stream into cache entry `gs`.
+}  // namespace gell
+
 static gell_status capture_step_graph(gell_ctx* c, gell_ctx::StepGraph& gs, int substeps) {
     if (gs.exec) {
         cudaGraphExecDestroy(gs.exec);

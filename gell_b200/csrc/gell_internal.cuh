@@ -112,6 +112,7 @@ struct gell_ctx {
     std::vector<gell::Substrate> subs;
     bool rate_valid = false;
     bool exact_chain = false;  // GELL_OPT_EXACT_CHAIN
+    int sweep_warps = 0;       // GELL_OPT_SWEEP_WARPS (0: as many as shared memory allows)
 
     // gell_run_mechanics: captured graphs of two mechanics steps and what each was captured for
     // (two entries: an odd number of steps flips the double buffers to the other assignment)
@@ -249,6 +250,14 @@ inline int blocks_for(long long n, int threads) {
 gell_status lod_solver(gell_ctx* c, int sub, int substeps);
 gell_status prelod(gell_ctx* c, int sub);
 gell_status fm_update(gell_ctx* c);
+// one mechanics step (fm_update, prelod of all substrates, `substeps` LOD substeps) on c->stream
+gell_status one_mechanics_step(gell_ctx* c, int substeps);
+// which buffer of each double-buffered cell field is current (a captured step is only valid for
+// the assignment it was captured with)
+uint32_t buffer_parity(const gell_ctx* c);
+// work that uses the cells waits for queued transfers first, and marks where the next one starts
+gell_status cells_begin(gell_ctx* c);
+gell_status cells_end(gell_ctx* c, gell_status st);
 gell_status birth(gell_ctx* c, int* n_out);
 gell_status death(gell_ctx* c, int* n_out);
 gell_status init_xorwow(gell_ctx* c);

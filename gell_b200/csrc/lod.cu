@@ -794,6 +794,7 @@ gell_status lod_solver(gell_ctx* c, int sub, int substeps) {
     const int fixed = 1024 + align128(ns * Na * 4) + 2 * 8 * 32 * 8;
     int w = (smem_cap - fixed) / (B * kSlotFloats * 4);
     w = w > kMaxComputeWarps ? kMaxComputeWarps : w;
+    if (c->sweep_warps > 0 && w > c->sweep_warps) w = c->sweep_warps;
     if (w < 1) return fail(c, GELL_ERR_UNSUPPORTED, "grid edge too large for the shared-memory line tiles");
     const int smem = 1024 + w * B * kSlotFloats * 4 + align128(ns * Na * 4) + 2 * w * 32 * 8;
     static bool configured = false;
@@ -806,12 +807,20 @@ gell_status lod_solver(gell_ctx* c, int sub, int substeps) {
     const long long xt = ((long long)N * N + 31) / 32 * ns;
     const long long yt = (long long)((c->g.P + 31) / 32) * N * ns;
     const long long zt = (c->g.PN + 31) / 32 * ns;
-    auto grid = [&](long long tiles) {
+    // as many CTAs as the tiles need, up to what can be resident at once (one per SM for large grids;
+    // several for small ones, whose CTAs need less shared memory)
+    auto grid = [&](long long tiles, const void* kern) {
+        int occ = 1;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, w * 64, smem) != cudaSuccess || occ < 1) {
+            cudaGetLastError();
+            occ = 1;
+        }
         long long want = (tiles + w - 1) / w;
-        long long cap = num_sms();
+        long long cap = (long long)num_sms() * occ;
         return (int)(want < cap ? want : cap);
     };
-    const int gx = grid(xt), gy = grid(yt), gz = grid(zt);
+    const int gx = grid(xt, (const void*)k_sweep<0>), gy = grid(yt, (const void*)k_sweep<1>),
+              gz = grid(zt, (const void*)k_sweep<2>);
     SrcArgs sa{};
     for (int s = s0; s < s1; ++s) {
         const Substrate& S = c->subs[s];

@@ -267,7 +267,10 @@ gell_status gell_sort_keys_noalloc(const int32_t* keys, int32_t* sorted_keys, in
 /* Options (none has a reference counterpart).  GELL_OPT_EXACT_CHAIN = 1 makes the LOD back
  * substitution run the exact division chain for every group instead of the speculative chain that
  * is checked against it; results are identical either way, this only makes the exact path testable. */
-enum { GELL_OPT_EXACT_CHAIN = 1 };
+enum { GELL_OPT_EXACT_CHAIN = 1, GELL_OPT_SWEEP_WARPS = 3 };
+/* GELL_OPT_SWEEP_WARPS (0..4, default 0): line tiles (compute warps) per CTA of the LOD sweeps;
+ * 0 = as many as shared memory holds.  Fewer give more, smaller CTAs, which can fill the GPU
+ * better for small grids run side by side (the ensemble tuner tries them).  Results do not change. */
 gell_status gell_set_option(gell_ctx* ctx, int option, int64_t value);
 
 /*
@@ -303,6 +306,29 @@ gell_status gell_checkpoint_load(gell_ctx* ctx, const char* path);
  * never seeds it, which is seed 1), computed by a private copy of that generator.  Host only.
  */
 gell_status gell_reference_spheroid(const gell_params* p, int n, float cell_radius, uint32_t seed, gell_cell* out);
+
+/*
+ * Ensembles: independent simulations stepped together (no counterpart in the reference, which runs
+ * one tumour per process).  Members are ordinary contexts on the same device, each with its own
+ * grid, cells and substrates.  gell_ensemble_run_mechanics runs `steps` mechanics steps of every
+ * member: pairs of steps replay ONE captured CUDA graph in which the members run on `branches`
+ * parallel streams, so the small kernels of many small grids share the GPU.  The graph is captured
+ * again when a member's cell count, substrates or buffer assignment, the substep count or the
+ * configuration changed.  Each member's own stream is ordered before and after the ensemble's work;
+ * biology steps and transfers stay per member (gell_cell_birth / gell_cell_death, ...).
+ * gell_ensemble_configure sets the branch count (1..64) and the sweeps' line tiles per CTA
+ * (GELL_OPT_SWEEP_WARPS, 0..4) of every member.  gell_ensemble_tune times branch counts 1, 2, 4, ..
+ * and tile widths 0, 2, 1 with real steps of the members (2 per trial, plus one first step; the
+ * total is returned in *steps_taken) and keeps the fastest.
+ */
+typedef struct gell_ensemble gell_ensemble;
+gell_status gell_ensemble_create(gell_ctx* const* members, int count, gell_ensemble** out);
+gell_status gell_ensemble_destroy(gell_ensemble* ens);
+gell_status gell_ensemble_configure(gell_ensemble* ens, int branches, int sweep_warps);
+gell_status gell_ensemble_run_mechanics(gell_ensemble* ens, int steps, int substeps);
+gell_status gell_ensemble_tune(gell_ensemble* ens, int substeps, int* steps_taken, int* best_branches,
+                               int* best_sweep_warps);
+gell_status gell_ensemble_sync(gell_ensemble* ens);
 
 /* Number of kernels this context has launched (always counted). */
 gell_status gell_launch_count(gell_ctx* ctx, int64_t* count);

@@ -1,0 +1,83 @@
+"""Ensembles (gell_ensemble_*): independent simulations of different sizes stepped together through
+one CUDA graph of parallel branches must give exactly what each gives when stepped alone, before
+and after the tuner and across birth and death (which re-captures the graph)."""
+import numpy as np
+import pytest
+
+from cases import ball_cells, random_field
+from gell_b200.cells import CELL_DTYPE
+
+pytestmark = pytest.mark.gpu
+
+gb = pytest.importorskip("gell_b200")
+
+SIZES = [(32, 1500), (40, 3000), (48, 800), (56, 5000), (64, 2500)]
+
+
+def raw(c):
+    return np.ascontiguousarray(c).view(np.uint8).reshape(len(c), CELL_DTYPE.itemsize)
+
+
+def member(i, N, n):
+    sim = gb.Simulation(voxel_num=N, voxel_length=10.0, max_cell_num=65536, rng_mode=gb.GELL_RNG_PHILOX, seed=100 + i)
+    D = 5e4 + 3e4 * i
+    sim.add_substrate(gb.Substrate(boundary=38.0, diffusion=D, decay=0.1, uptake=-(5.0 + 3.0 * i), init=38.0))
+    sim.set_field(0, random_field(N, seed=200 + i))
+    cells = gb.seed_ki67_states(ball_cells(N, 10.0, n, seed=300 + i, radius_frac=0.3, outside=0), 400 + i)
+    sim.import_cells(cells)
+    return sim
+
+
+def state(sim):
+    return raw(sim.export_cells()), sim.field(0).view(np.uint32)
+
+
+def members():
+    return [member(i, N, n) for i, (N, n) in enumerate(SIZES)]
+
+
+def test_ensemble_matches_members_stepped_alone():
+    alone = members()
+    for m in alone:
+        for _ in range(5):
+            m.mechanics_step(4)
+    together = members()
+    with gb.Ensemble(together) as ens:
+        ens.configure(branches=3, sweep_warps=2)
+        ens.run_mechanics(5, 4)
+        ens.sync()
+    for a, b in zip(alone, together):
+        for x, y in zip(state(a), state(b)):
+            np.testing.assert_array_equal(x, y)
+        assert a.launch_count() == b.launch_count()
+    for m in alone + together:
+        m.close()
+
+
+def test_ensemble_across_birth_and_death_and_tuning():
+    alone = members()
+    together = members()
+    with gb.Ensemble(together) as ens:
+        taken, branches, warps = ens.tune(3)
+        assert taken >= 3 and 1 <= branches <= len(SIZES) and warps in (0, 1, 2)
+        for m in alone:
+            for _ in range(taken):
+                m.mechanics_step(3)
+        for _ in range(2):
+            for a, b in zip(alone, together):
+                a.CellBirth_kernel()
+                b.CellBirth_kernel()
+            for a in alone:
+                for _ in range(4):
+                    a.mechanics_step(3)
+            ens.run_mechanics(4, 3)
+            for a, b in zip(alone, together):
+                a.CellDeath_kernel()
+                b.CellDeath_kernel()
+        ens.sync()
+    for a, b in zip(alone, together):
+        assert a.count() == b.count()
+        for x, y in zip(state(a), state(b)):
+            np.testing.assert_array_equal(x, y)
+    for m in alone + together:
+        m.close()
