@@ -402,6 +402,115 @@ def run_c3(args, rank, world, local_rank):
     return line
 
 
+# ---------------------------------------------------------------------------- ensemble workload
+
+C4_MEMBERS, C4_BIO = 64, 60
+C4_WORKLOAD = ("batched ensemble: 64 independent instances, grid edge log-uniform in [64, 200] voxels of 10 um, "
+               "cells log-uniform in [2,000, 200,000], D U(5e4, 2e5), uptake U(5, 20)/min (seed 7), one FP32 "
+               "substrate each, Philox birth/death; one graph of parallel branches, tuned")
+
+
+def c4_members(gb, stream):
+    rng = np.random.Generator(np.random.Philox(7))
+    edges = np.floor(np.exp(rng.uniform(np.log(64), np.log(200), C4_MEMBERS))).astype(int)
+    cells = np.floor(np.exp(rng.uniform(np.log(2e3), np.log(2e5), C4_MEMBERS))).astype(int)
+    D = rng.uniform(5e4, 2e5, C4_MEMBERS)
+    up = rng.uniform(5.0, 20.0, C4_MEMBERS)
+    sims = []
+    for i in range(C4_MEMBERS):
+        N = int(edges[i])
+        # at most 35% of the domain's volume packed at 0.6, so the spheroid (radius 0.44 of the
+        # edge) stays inside the grid
+        n = int(min(cells[i], 0.35 * (N * LENGTH) ** 3 / 873.0))
+        sim = gb.Simulation(voxel_num=N, voxel_length=LENGTH, max_cell_num=2 * n + 1024,
+                            rng_mode=gb.GELL_RNG_PHILOX, seed=1000 + i)
+        sim.add_substrate(gb.Substrate(38.0, float(D[i]), 0.1, -float(up[i]), 38.0))
+        c = gb.lattice_spheroid(n, N * LENGTH / 2, i, LENGTH, N)
+        gb.seed_ki67_states(c, 2000 + i)
+        sim.import_cells(c)
+        sim.set_stream(stream)
+        sims.append(sim)
+    return sims, edges
+
+
+def run_c4(args, rank, world, local_rank):
+    """--workload c4: K mechanics steps of all members in biology periods of 60."""
+    import torch
+    import gell_b200 as gb
+
+    torch.cuda.set_device(local_rank)
+    stream = torch.cuda.Stream()
+    sims, edges = c4_members(gb, stream)
+    ens = gb.Ensemble(sims)
+    taken, branches, warps = ens.tune(SUBSTEPS)
+    ens.run_mechanics(max(0, args.warmup - taken) + 2, SUBSTEPS)
+    ens.sync()
+    ncells0 = sum(s.count() for s in sims)
+
+    # the same members stepped one after another (per-member calls), for comparison
+    torch.cuda.synchronize()
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    q0.record(stream)
+    for sim in sims:
+        sim.mechanics_step(SUBSTEPS)
+    q1.record(stream)
+    torch.cuda.synchronize()
+    t_seq_step = q0.elapsed_time(q1)
+
+    props = torch.cuda.get_device_properties(local_rank)
+    uuid = getattr(props, "uuid", None)
+    uuid = f"GPU-{uuid}" if uuid is not None and not str(uuid).startswith("GPU-") else uuid
+    sampler = ClockSampler(str(uuid) if uuid else None)
+    sampler.start()
+    time.sleep(0.3)
+    K = args.steps
+    cell_steps = 0
+    launches0 = sum(s.launch_count() for s in sims)
+    if world > 1:
+        import torch.distributed as td
+        td.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    done = 0
+    while done < K:
+        m = min(C4_BIO, K - done)
+        n_after_birth = sum(s.CellBirth_kernel() for s in sims)
+        ens.run_mechanics(m, SUBSTEPS)
+        for s in sims:
+            s.CellDeath_kernel()
+        cell_steps += n_after_birth * m
+        done += m
+    e1.record(stream)
+    torch.cuda.synchronize()
+    sampler.stop()
+    t_all = e0.elapsed_time(e1)
+    launches = sum(s.launch_count() for s in sims) - launches0
+    times = np.array([t_all], np.float64)
+    cnt = np.array([cell_steps], np.float64)
+    if world > 1:
+        times, cnt = reduce_over_ranks(times, cnt, "cuda")
+    line = None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": cnt[0] / (times[0] / 1e3), "unit": "cell-updates/s", "n_gpus": world,
+            "steps": K, "warmup": args.warmup, "ms_per_step": times[0] / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: 64 seeded jittered-lattice spheroids with seeded Ki-67 states",
+            "config": {"workload": C4_WORKLOAD, "members": C4_MEMBERS, "voxels_total": int((edges ** 3).sum()),
+                       "cells_total_start": int(ncells0), "substeps_per_step": SUBSTEPS,
+                       "biology_period_steps": C4_BIO, "tuned_branches": branches, "tuned_sweep_warps": warps,
+                       "tuning_steps": taken, "parallelism": "replicas"},
+            "components": {"ms_per_step_members_one_by_one": t_seq_step,
+                           "speedup_vs_members_one_by_one": t_seq_step / (times[0] / K)},
+            "gpu_launches": int(launches), "clocks": sampler.summary(),
+        }
+    ens.close()
+    for sim in sims:
+        sim.close()
+    return line
+
+
 # ---------------------------------------------------------------------------- CPU (oracle) leg
 
 class CpuWork:
@@ -489,8 +598,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("gell", "reference"), default="gell")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=("large", "c3"), default="large",
-                    help="large: 400^3, 10^6 cells (the headline line); c3: 600^3, 5*10^6 cells with birth/death")
+    ap.add_argument("--workload", choices=("large", "c3", "c4"), default="large",
+                    help="large: 400^3, 10^6 cells (the headline line); c3: 600^3, 5*10^6 cells with "
+                         "birth/death; c4: ensemble of 64 small instances")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -510,8 +620,8 @@ def main():
         import torch.distributed as td
         torch.cuda.set_device(local_rank)
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    if args.workload == "c3":
-        line = run_c3(args, rank, world, local_rank)
+    if args.workload in ("c3", "c4"):
+        line = (run_c3 if args.workload == "c3" else run_c4)(args, rank, world, local_rank)
         if rank == 0:
             print(json.dumps(line), flush=True)
         if world > 1:
