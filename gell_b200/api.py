@@ -149,13 +149,14 @@ def load_library() -> ctypes.CDLL:
     L.gell_profile_read.argtypes = [P, P, ctypes.c_int, P, ctypes.c_int]
     L.gell_launch_count.argtypes = [P, P]
     L.gell_set_option.argtypes = [P, ctypes.c_int, ctypes.c_int64]
+    L.gell_selftest_timeout.argtypes = [P, ctypes.c_int]
     L.gell_selftest_division.argtypes = [P, ctypes.c_int64, ctypes.c_uint64, P]
     for name in ("gell_create", "gell_destroy", "gell_set_stream", "gell_substrate_add",
                  "gell_cells_import", "gell_cells_export", "gell_cell_count", "gell_field_import",
                  "gell_field_export", "gell_fm_update", "gell_prelod", "gell_lod_solver",
                  "gell_cell_birth", "gell_cell_death", "gell_mechanics_step", "gell_sync",
                  "gell_debug_dump", "gell_profile_enable", "gell_profile_read", "gell_launch_count",
-                 "gell_selftest_division", "gell_set_option", "gell_cells_import_async",
+                 "gell_selftest_division", "gell_set_option", "gell_selftest_timeout", "gell_cells_import_async",
                  "gell_cells_export_async", "gell_wait_transfers", "gell_run_mechanics",
                  "gell_write_cells_csv", "gell_save_cells_csv", "gell_save_field_csv",
                  "gell_save_field_slice_csv", "gell_checkpoint_save", "gell_checkpoint_load",
@@ -361,6 +362,10 @@ class Simulation:
         self._check(self.lib.gell_selftest_division(self.h, samples, seed, ctypes.byref(m)),
                     "gell_selftest_division")
         return m.value
+
+    def selftest_timeout(self, polls: int = 1000) -> int:
+        """Run the bounded-wait give-up path; returns the status (GELL_ERR_TIMEOUT = -5 expected)."""
+        return self.lib.gell_selftest_timeout(self.h, polls)
 
     def set_exact_chain(self, on: bool = True) -> None:
         """Run every LOD back-substitution group on the exact division chain (same results)."""

@@ -316,7 +316,11 @@ gell_status gell_sync(gell_ctx* c) {
     if (c->xfer_pending) GELL_CUDA(c, cudaStreamSynchronize(c->xfer));
     int herr = 0;
     GELL_CUDA(c, cudaMemcpy(&herr, c->dev_err, 4, cudaMemcpyDeviceToHost));
-    if (herr) return fail(c, GELL_ERR_TIMEOUT, "a bounded device wait gave up (code " + std::to_string(herr) + ")");
+    if (herr) {
+        // reported once: the word is cleared so that the context can go on
+        GELL_CUDA(c, cudaMemset(c->dev_err, 0, 4));
+        return fail(c, GELL_ERR_TIMEOUT, "a bounded device wait gave up (code " + std::to_string(herr) + ")");
+    }
     return GELL_OK;
 }
 
@@ -480,6 +484,7 @@ gell_status cells_end(gell_ctx* c, gell_status st) {
 extern "C" {
 
 gell_status gell_cells_import(gell_ctx* c, const gell_cell* cells, int n, int on_device) {
+    GELL_RANGE("gell_cells_import");
     if (!c || (n > 0 && !cells) || n < 0) return GELL_ERR_INVALID_ARG;
     if (gell_status b = cells_begin(c)) return b;
     if (n > c->cap) return fail(c, GELL_ERR_CAPACITY, "more cells than max_cell_num");
@@ -499,6 +504,7 @@ gell_status gell_cells_import(gell_ctx* c, const gell_cell* cells, int n, int on
 }
 
 gell_status gell_cells_export(gell_ctx* c, gell_cell* cells, int capacity, int* n_out, int on_device) {
+    GELL_RANGE("gell_cells_export");
     if (!c || (c->n > 0 && !cells)) return GELL_ERR_INVALID_ARG;
     if (capacity < c->n) return fail(c, GELL_ERR_CAPACITY, "export buffer too small");
     if (gell_status b = cells_begin(c)) return b;
@@ -517,6 +523,7 @@ gell_status gell_cells_export(gell_ctx* c, gell_cell* cells, int capacity, int* 
 }
 
 gell_status gell_cells_import_async(gell_ctx* c, const gell_cell* cells, int n) {
+    GELL_RANGE("gell_cells_import_async");
     if (!c || (n > 0 && !cells) || n < 0) return GELL_ERR_INVALID_ARG;
     if (n > c->cap) return fail(c, GELL_ERR_CAPACITY, "more cells than max_cell_num");
     GELL_CUDA(c, cudaStreamWaitEvent(c->xfer, c->cells_ev, 0));
@@ -536,6 +543,7 @@ gell_status gell_cells_import_async(gell_ctx* c, const gell_cell* cells, int n) 
 }
 
 gell_status gell_cells_export_async(gell_ctx* c, gell_cell* cells, int capacity, int* n_out) {
+    GELL_RANGE("gell_cells_export_async");
     if (!c || (c->n > 0 && !cells)) return GELL_ERR_INVALID_ARG;
     if (capacity < c->n) return fail(c, GELL_ERR_CAPACITY, "export buffer too small");
     const int n = c->n;
@@ -640,6 +648,12 @@ gell_status gell_selftest_division(gell_ctx* c, int64_t samples, uint64_t seed, 
     return st;
 }
 
+gell_status gell_selftest_timeout(gell_ctx* c, int polls) {
+    if (!c || polls < 1) return GELL_ERR_INVALID_ARG;
+    if (gell_status st = selftest_timeout(c, polls)) return st;
+    return gell_sync(c);
+}
+
 gell_status gell_set_option(gell_ctx* c, int option, int64_t value) {
     if (!c) return GELL_ERR_INVALID_ARG;
     switch (option) {
@@ -659,35 +673,41 @@ gell_status gell_launch_count(gell_ctx* c, int64_t* count) {
 }
 
 gell_status gell_fm_update(gell_ctx* c) {
+    GELL_RANGE("gell_fm_update");
     if (!c) return GELL_ERR_INVALID_ARG;
     if (gell_status b = cells_begin(c)) return b;
     return cells_end(c, fm_update(c));
 }
 
 gell_status gell_prelod(gell_ctx* c, int sub) {
+    GELL_RANGE("gell_prelod");
     if (!c || sub < -1 || sub >= (int)c->subs.size()) return GELL_ERR_INVALID_ARG;
     if (gell_status b = cells_begin(c)) return b;
     return cells_end(c, prelod(c, sub));
 }
 
 gell_status gell_lod_solver(gell_ctx* c, int sub, int substeps) {
+    GELL_RANGE("gell_lod_solver");
     if (!c || sub < -1 || sub >= (int)c->subs.size() || substeps < 0) return GELL_ERR_INVALID_ARG;
     return lod_solver(c, sub, substeps);
 }
 
 gell_status gell_cell_birth(gell_ctx* c, int* n_out) {
+    GELL_RANGE("gell_cell_birth");
     if (!c) return GELL_ERR_INVALID_ARG;
     if (gell_status b = cells_begin(c)) return b;
     return cells_end(c, birth(c, n_out));
 }
 
 gell_status gell_cell_death(gell_ctx* c, int* n_out) {
+    GELL_RANGE("gell_cell_death");
     if (!c) return GELL_ERR_INVALID_ARG;
     if (gell_status b = cells_begin(c)) return b;
     return cells_end(c, death(c, n_out));
 }
 
 gell_status gell_mechanics_step(gell_ctx* c, int substeps) {
+    GELL_RANGE("gell_mechanics_step");
     if (!c || substeps < 0) return GELL_ERR_INVALID_ARG;
     if (gell_status b = cells_begin(c)) return b;
     gell_status s = fm_update(c);
@@ -755,6 +775,7 @@ static gell_status capture_step_graph(gell_ctx* c, gell_ctx::StepGraph& gs, int 
 extern "C" {
 
 gell_status gell_run_mechanics(gell_ctx* c, int steps, int substeps) {
+    GELL_RANGE("gell_run_mechanics");
     if (!c || steps < 0 || substeps < 0) return GELL_ERR_INVALID_ARG;
     if (steps == 0) return GELL_OK;
     if (gell_status b = cells_begin(c)) return b;

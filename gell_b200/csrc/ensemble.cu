@@ -192,6 +192,7 @@ gell_status gell_ensemble_configure(gell_ensemble* e, int branches, int sweep_wa
 }
 
 gell_status gell_ensemble_run_mechanics(gell_ensemble* e, int steps, int substeps) {
+    GELL_RANGE("gell_ensemble_run_mechanics");
     if (!e || steps < 0 || substeps < 0) return GELL_ERR_INVALID_ARG;
     if (steps == 0) return GELL_OK;
     int left = steps;

@@ -16,6 +16,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <curand_kernel.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
 #include <string>
@@ -186,6 +187,14 @@ gell_status cuda_fail(gell_ctx* c, cudaError_t e, const char* where);
         if (e_ != cudaSuccess) return gell::cuda_fail(ctx, e_, what);  \
     } while (0)
 
+// An NVTX range around an entry point, for timeline tools (header-only NVTX 3: free when no tool
+// is attached).
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+};
+#define GELL_RANGE(name) gell::NvtxRange gell_range_(name)
+
 // Every kernel launch goes through GELL_KERNEL: it is counted, timed when profiling is on, and
 // its launch error is turned into a status.
 int prof_begin(gell_ctx* c, const char* name);
@@ -250,6 +259,7 @@ inline int blocks_for(long long n, int threads) {
 gell_status lod_solver(gell_ctx* c, int sub, int substeps);
 gell_status prelod(gell_ctx* c, int sub);
 gell_status fm_update(gell_ctx* c);
+gell_status selftest_timeout(gell_ctx* c, int polls);
 // one mechanics step (fm_update, prelod of all substrates, `substeps` LOD substeps) on c->stream
 gell_status one_mechanics_step(gell_ctx* c, int substeps);
 // which buffer of each double-buffered cell field is current (a captured step is only valid for

@@ -143,6 +143,7 @@ gell_status gell_save_field_slice_csv(gell_ctx* c, int substrate, const char* pa
 // epoch and biology step, the cells (72-byte records), every field (N^3 floats, x fastest), and
 // with XORWOW draws the generator state of every slot.
 gell_status gell_checkpoint_save(gell_ctx* c, const char* path) {
+    GELL_RANGE("gell_checkpoint_save");
     if (!c || !path) return GELL_ERR_INVALID_ARG;
     if (gell_status st = gell_sync(c)) return st;
     const int32_t nsub = (int32_t)c->subs.size(), n = c->n;
@@ -175,6 +176,7 @@ gell_status gell_checkpoint_save(gell_ctx* c, const char* path) {
 }
 
 gell_status gell_checkpoint_load(gell_ctx* c, const char* path) {
+    GELL_RANGE("gell_checkpoint_load");
     if (!c || !path) return GELL_ERR_INVALID_ARG;
     File in(path, "rb");
     if (!in.f) return fail(c, GELL_ERR_INVALID_ARG, "cannot open the checkpoint file");

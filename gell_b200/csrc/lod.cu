@@ -103,8 +103,8 @@ __device__ __forceinline__ bool mbar_wait1(uint64_t* b, uint32_t parity, int* er
 // Bounded, warp-uniform wait on an mbarrier phase: every lane polls until all lanes see the phase
 // complete; after a fixed number of polls the warp gives up together, records `code` in the
 // context's error word and returns false (the host then reports GELL_ERR_TIMEOUT).
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, int* err, int code) {
-    for (int it = 0; it < (1 << 22); ++it)
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, int* err, int code, int limit = 1 << 22) {
+    for (int it = 0; it < limit; ++it)
         if (__all_sync(FULL, mbar_try_wait(b, parity))) return true;
     if ((threadIdx.x & 31) == 0) atomicExch(err, code);
     return false;
@@ -614,6 +614,17 @@ __global__ void __launch_bounds__(64 * kMaxComputeWarps, 1) k_sweep(const __grid
     }
 }
 
+// The bounded wait's give-up path: nothing ever arrives on this barrier, so the wait must stop after
+// `polls` polls and record code 12 in the context's error word, as a sweep does when a box never
+// lands.  Run by gell_selftest_timeout; the context stays usable afterwards.
+__global__ void k_wait_check(int polls, int* err) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) mbar_init(&bar, 1u);
+    fence_mbar_init();
+    __syncthreads();
+    mbar_wait(&bar, 0u, err, 12, polls);
+}
+
 // Markstein division against IEEE division on random operands in the sweeps' range.
 __global__ void k_div_check(long long n, unsigned long long seed, unsigned long long* bad) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -839,6 +850,11 @@ gell_status lod_solver(gell_ctx* c, int sub, int substeps) {
         GELL_KERNEL(c, "k_sweep_y", k_sweep<1><<<gy, w * 64, smem, c->stream>>>(ay));
         GELL_KERNEL(c, "k_sweep_z", k_sweep<2><<<gz, w * 64, smem, c->stream>>>(az));
     }
+    return GELL_OK;
+}
+
+gell_status selftest_timeout(gell_ctx* c, int polls) {
+    GELL_KERNEL(c, "k_wait_check", k_wait_check<<<1, 32, 0, c->stream>>>(polls, c->dev_err));
     return GELL_OK;
 }
 

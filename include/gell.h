@@ -245,6 +245,12 @@ gell_status gell_profile_read(gell_ctx* ctx, gell_profile_record* out, int max_r
  * range; *mismatches = number of quotients that differ in any bit.  Synchronises. */
 gell_status gell_selftest_division(gell_ctx* ctx, int64_t samples, uint64_t seed, int64_t* mismatches);
 
+/* Self-test of the bounded device waits: a kernel waits on a barrier that nothing completes, gives
+ * up after `polls` polls and records it, so this returns GELL_ERR_TIMEOUT (reported once; the
+ * context stays usable).  This is the path a sweep takes when a TMA box never lands.  No
+ * counterpart in the reference, which has no device-side waits. */
+gell_status gell_selftest_timeout(gell_ctx* ctx, int polls);
+
 /* Largest key count gell_sort_keys_noalloc accepts. */
 #define GELL_NOALLOC_MAX_KEYS (1 << 20)
 

@@ -60,3 +60,43 @@ def test_reference_arm_runs_on_rank_zero_only():
                         "--steps", "1", "--warmup", "3"], env=env, capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stderr
     assert r.stdout.strip() == ""
+
+
+def _rank_dies(rank, world, port, out):
+    import datetime
+
+    import torch.distributed as td
+    sys.path.insert(0, ROOT)
+    import bench
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    td.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=10))
+    if rank == 1:
+        os._exit(3)  # this replica dies before the reduction
+    import time
+    t0 = time.time()
+    try:
+        bench.reduce_over_ranks(np.ones(4), np.ones(2), "cpu")
+        out[rank] = "no error"
+    except Exception as e:  # the survivor sees an error instead of waiting for ever
+        out[rank] = f"error after {time.time() - t0:.1f}s: {type(e).__name__}"
+    os._exit(0)
+
+
+def test_a_dead_replica_makes_the_reduction_fail_not_hang():
+    world = 2
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as m:
+        out = m.dict()
+        port = _free_port()
+        procs = [ctx.Process(target=_rank_dies, args=(r, world, port, out)) for r in range(world)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(timeout=120)
+        alive = [p for p in procs if p.is_alive()]
+        for p in alive:
+            p.kill()
+        assert not alive, "a rank hung"
+        res = dict(out)
+    assert res.get(0, "").startswith("error after"), res
