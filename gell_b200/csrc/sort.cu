@@ -80,15 +80,69 @@ __global__ void __launch_bounds__(1024) k_scan_single(uint32_t* a, long long m, 
     if (total && t == 1023) *total = (int)(warp_sums[31]);
 }
 
+// Exclusive scan of one digit's per-tile counts (row d of the digit-major table), in place, by
+// CTA d; the digit's total goes to totals[d].  The scatter adds the prefix of the totals.
+__global__ void __launch_bounds__(kThreads) k_digit_scan(uint32_t* __restrict__ hist, int nb,
+                                                         uint32_t* __restrict__ totals) {
+    __shared__ uint32_t ws[kThreads / 32];
+    uint32_t* row = hist + (long long)blockIdx.x * nb;
+    const int per = (nb + kThreads - 1) / kThreads;
+    const int lo = threadIdx.x * per, hi = lo + per < nb ? lo + per : nb;
+    uint32_t s = 0;
+    for (int i = lo; i < hi; ++i) s += row[i];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t x = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) ws[w] = x;
+    __syncthreads();
+    uint32_t wpre = 0;
+    for (int j = 0; j < w; ++j) wpre += ws[j];
+    uint32_t run = wpre + x - s;
+    for (int i = lo; i < hi; ++i) {
+        const uint32_t v = row[i];
+        row[i] = run;
+        run += v;
+    }
+    if (threadIdx.x == kThreads - 1) totals[blockIdx.x] = run;
+}
+
 __global__ void __launch_bounds__(kThreads) k_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                                                       uint32_t* __restrict__ kout, uint32_t* __restrict__ vout, int n,
                                                       int shift, int R, const uint32_t* __restrict__ offs, int nb,
-                                                      int iota) {
+                                                      const uint32_t* __restrict__ totals, int iota) {
     __shared__ uint32_t wcnt[kThreads / 32][256];
     __shared__ uint32_t gbase[256];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < (kThreads / 32) * 256; i += kThreads) (&wcnt[0][0])[i] = 0;
-    for (int d = threadIdx.x; d < R; d += kThreads) gbase[d] = offs[(long long)d * nb + blockIdx.x];
+    if (w == 0) {
+        // exclusive prefix of the digit totals: lane l sums digits 8l .. 8l+7 (R <= 256)
+        uint32_t t[8], s = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int d = 8 * lane + k;
+            t[k] = d < R ? totals[d] : 0u;
+            s += t[k];
+        }
+        uint32_t x = s;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(FULL, x, o);
+            if (lane >= o) x += y;
+        }
+        uint32_t run = x - s;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int d = 8 * lane + k;
+            if (d < R) gbase[d] = run;
+            run += t[k];
+        }
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < R; d += kThreads) gbase[d] += offs[(long long)d * nb + blockIdx.x];
     __syncthreads();
     const uint32_t mask = (uint32_t)R - 1u;
     const long long base = (long long)blockIdx.x * kTile + w * (kTile / (kThreads / 32));
@@ -187,7 +241,8 @@ __global__ void __launch_bounds__(kThreads) k_tile_scan(const uint32_t* __restri
 
 }  // namespace
 
-size_t sort_hist_entries(int cap) { return (size_t)256 * ((cap + kTile - 1) / kTile) + 64; }
+// digit-major count table, then the 256 digit totals
+size_t sort_hist_entries(int cap) { return (size_t)256 * ((cap + kTile - 1) / kTile) + 256 + 64; }
 
 gell_status radix_sort(gell_ctx* c, int n, int bits, bool vals_are_iota) {
     SortScratch& S = c->sort;
@@ -205,9 +260,10 @@ gell_status radix_sort(gell_ctx* c, int n, int bits, bool vals_are_iota) {
     for (int p = 0; p < passes; ++p) {
         const int shift = p * d;
         GELL_KERNEL(c, "k_hist", k_hist<<<nb, kThreads, 0, c->stream>>>(S.keys[in], n, shift, R, S.hist, nb));
-        GELL_KERNEL(c, "k_scan_single", k_scan_single<<<1, 1024, 0, c->stream>>>(S.hist, (long long)R * nb, nullptr));
+        uint32_t* totals = S.hist + (size_t)R * nb;
+        GELL_KERNEL(c, "k_digit_scan", k_digit_scan<<<R, kThreads, 0, c->stream>>>(S.hist, nb, totals));
         GELL_KERNEL(c, "k_scatter", k_scatter<<<nb, kThreads, 0, c->stream>>>(S.keys[in], S.vals[in], S.keys[in ^ 1], S.vals[in ^ 1], n, shift,
-                                                   R, S.hist, nb, iota ? 1 : 0));
+                                                   R, S.hist, nb, totals, iota ? 1 : 0));
         iota = false;
         in ^= 1;
     }
