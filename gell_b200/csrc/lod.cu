@@ -701,16 +701,20 @@ struct PreArgs {
 
 // Clear the lines flagged by the previous map (oxy_consumption_reset, include/LODkernel.cuh:183-190,
 // restricted to the lines that can be nonzero).
+// One warp per listed line: the row (P floats, P a multiple of 4) is cleared with 16-byte stores.
 __global__ void k_rate_reset(PreArgs a) {
-    const int P = a.g.P;
+    const int P4 = a.g.P >> 2;
+    const int lane = threadIdx.x & 31;
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int s = 0; s < a.nsub; ++s) {
         const int cnt = *a.count[s];
-        for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < (long long)cnt * P;
-             w += (long long)gridDim.x * blockDim.x) {
-            const int li = (int)(w / P), x = (int)(w - (long long)li * P);
+        for (long long li = gw; li < cnt; li += nw) {
             const int line = a.list[s][li];
-            a.rate[s][(long long)line * P + x] = 0.f;
-            if (x == 0) a.flag[s][line] = 0;
+            float4* row = reinterpret_cast<float4*>(a.rate[s] + (long long)line * a.g.P);
+            for (int x4 = lane; x4 < P4; x4 += 32) row[x4] = z;
+            if (lane == 0) a.flag[s][line] = 0;
         }
     }
 }
