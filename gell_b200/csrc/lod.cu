@@ -812,12 +812,13 @@ gell_status lod_solver(gell_ctx* c, int sub, int substeps) {
     if (c->sweep_warps > 0 && w > c->sweep_warps) w = c->sweep_warps;
     if (w < 1) return fail(c, GELL_ERR_UNSUPPORTED, "grid edge too large for the shared-memory line tiles");
     const int smem = 1024 + w * B * kSlotFloats * 4 + align128(ns * Na * 4) + 2 * w * 32 * 8;
-    static bool configured = false;
-    if (!configured) {
+    // the shared-memory opt-in is a per-device function attribute: set once per context (each
+    // context lives on one device)
+    if (!c->sweeps_configured) {
         GELL_CUDA(c, cudaFuncSetAttribute(k_sweep<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
         GELL_CUDA(c, cudaFuncSetAttribute(k_sweep<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
         GELL_CUDA(c, cudaFuncSetAttribute(k_sweep<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
-        configured = true;
+        c->sweeps_configured = true;
     }
     const long long xt = ((long long)N * N + 31) / 32 * ns;
     const long long yt = (long long)((c->g.P + 31) / 32) * N * ns;
