@@ -298,7 +298,10 @@ gell_status gell_create(const gell_params* params, gell_ctx** out) {
 
 gell_status gell_destroy(gell_ctx* c) {
     if (!c) return GELL_ERR_INVALID_ARG;
+    // queued kernels, replayed graphs and transfers into the caller's host buffers finish first
     cudaStreamSynchronize(c->stream);
+    if (c->xfer) cudaStreamSynchronize(c->xfer);
+    if (c->own_stream && c->own_stream != c->stream) cudaStreamSynchronize(c->own_stream);
     free_all(c);
     delete c;
     return GELL_OK;
@@ -574,34 +577,41 @@ gell_status gell_cell_count(gell_ctx* c, int* n_out) {
 
 gell_status gell_field_import(gell_ctx* c, int sub, const float* field, int on_device) {
     if (!c || !field || sub < 0 || sub >= (int)c->subs.size()) return GELL_ERR_INVALID_ARG;
-    const float* src = field;
-    float* tmp = nullptr;
-    size_t bytes = (size_t)c->nvox * 4;
-    if (!on_device) {
-        GELL_CUDA(c, cudaMallocAsync((void**)&tmp, bytes, c->stream));
-        GELL_CUDA(c, cudaMemcpyAsync(tmp, field, bytes, cudaMemcpyHostToDevice, c->stream));
-        src = tmp;
+    const size_t bytes = (size_t)c->nvox * 4;
+    if (on_device) {
+        GELL_KERNEL(c, "k_field_in", k_field_in<<<blocks_for(c->nvox, 256), 256, 0, c->stream>>>(field, c->subs[sub].p, c->g));
+        return GELL_OK;
     }
-    GELL_KERNEL(c, "k_field_in", k_field_in<<<blocks_for(c->nvox, 256), 256, 0, c->stream>>>(src, c->subs[sub].p, c->g));
-    if (tmp) GELL_CUDA(c, cudaFreeAsync(tmp, c->stream));
+    // a dense staging copy on the device, freed in stream order on every path
+    float* tmp = nullptr;
+    GELL_CUDA(c, cudaMallocAsync((void**)&tmp, bytes, c->stream));
+    cudaError_t e = cudaMemcpyAsync(tmp, field, bytes, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) {
+        k_field_in<<<blocks_for(c->nvox, 256), 256, 0, c->stream>>>(tmp, c->subs[sub].p, c->g);
+        c->launches++;
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(tmp, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "gell_field_import");
     return GELL_OK;
 }
 
 gell_status gell_field_export(gell_ctx* c, int sub, float* field, int on_device) {
     if (!c || !field || sub < 0 || sub >= (int)c->subs.size()) return GELL_ERR_INVALID_ARG;
-    float* dst = field;
+    const size_t bytes = (size_t)c->nvox * 4;
+    if (on_device) {
+        GELL_KERNEL(c, "k_field_out", k_field_out<<<blocks_for(c->nvox, 256), 256, 0, c->stream>>>(c->subs[sub].p, field, c->g));
+        return GELL_OK;
+    }
     float* tmp = nullptr;
-    size_t bytes = (size_t)c->nvox * 4;
-    if (!on_device) {
-        GELL_CUDA(c, cudaMallocAsync((void**)&tmp, bytes, c->stream));
-        dst = tmp;
-    }
-    GELL_KERNEL(c, "k_field_out", k_field_out<<<blocks_for(c->nvox, 256), 256, 0, c->stream>>>(c->subs[sub].p, dst, c->g));
-    if (tmp) {
-        GELL_CUDA(c, cudaMemcpyAsync(field, tmp, bytes, cudaMemcpyDeviceToHost, c->stream));
-        GELL_CUDA(c, cudaFreeAsync(tmp, c->stream));
-        GELL_CUDA(c, cudaStreamSynchronize(c->stream));
-    }
+    GELL_CUDA(c, cudaMallocAsync((void**)&tmp, bytes, c->stream));
+    k_field_out<<<blocks_for(c->nvox, 256), 256, 0, c->stream>>>(c->subs[sub].p, tmp, c->g);
+    c->launches++;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(field, tmp, bytes, cudaMemcpyDeviceToHost, c->stream);
+    cudaFreeAsync(tmp, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "gell_field_export");
     return GELL_OK;
 }
 

@@ -325,7 +325,8 @@ gell_status gell_reference_spheroid(const gell_params* p, int n, float cell_radi
  * gell_ensemble_configure sets the branch count (1..64) and the sweeps' line tiles per CTA
  * (GELL_OPT_SWEEP_WARPS, 0..4) of every member.  gell_ensemble_tune times branch counts 1, 2, 4, ..
  * and tile widths 0, 2, 1 with real steps of the members (2 per trial, plus one first step; the
- * total is returned in *steps_taken) and keeps the fastest.
+ * total is returned in *steps_taken) and keeps the fastest.  The members must outlive the ensemble
+ * and live on the device that is current when it is created.
  */
 typedef struct gell_ensemble gell_ensemble;
 gell_status gell_ensemble_create(gell_ctx* const* members, int count, gell_ensemble** out);
