@@ -99,9 +99,10 @@ __global__ void __launch_bounds__(256) k_force_move(MechArgs a) {
     const int3 b = find_bin(pr.x, pr.y, pr.z, a.g.len);
     float fx = 0.f, fy = 0.f, fz = 0.f;
     float thres = a.max_dist;
-    // d >= thres is certain when |dp|^2 + 0.0001 (in double) exceeds thres^2 by a relative margin
-    // far above the roundings between it and d: such candidates skip the square root.
-    double thr_hi = (double)thres * (double)thres * (1.0 + 0x1p-20);
+    // d >= thres is certain when |dp|^2 alone exceeds thres^2 (1 + 2^-20), a relative margin far
+    // above the roundings between |dp|^2 + 0.0001 and d: such candidates skip the double-precision
+    // add and the square root.  The float threshold is that bound rounded up.
+    float thr_hi = __double2float_ru((double)thres * (double)thres * (1.0 + 0x1p-20));
     // the 27 bins in the reference's order: xi outer, then yi, then zi
 #pragma unroll 1
     for (int o = 0; o < 27; ++o) {
@@ -117,14 +118,13 @@ __global__ void __launch_bounds__(256) k_force_move(MechArgs a) {
             const float dy = __fsub_rn(pr.y, q.y);
             const float dz = __fsub_rn(pr.z, q.z);
             const float ss = __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
-            const double x = __dadd_rn((double)ss, 0.0001);
-            if (x > thr_hi) continue;
-            const float d = __fsqrt_rn(__double2float_rn(x));
+            if (ss > thr_hi) continue;
+            const float d = __fsqrt_rn(__double2float_rn(__dadd_rn((double)ss, 0.0001)));
             if (d >= thres) continue;
             const float rs = __fadd_rn(q.w, pr.w);
             const float R = rs > 0.01f ? rs : 0.01f;
             thres = __double2float_rn(__dmul_rn((double)R, a.ra_ratio));
-            thr_hi = (double)thres * (double)thres * (1.0 + 0x1p-20);
+            thr_hi = __double2float_ru((double)thres * (double)thres * (1.0 + 0x1p-20));
             if (d >= thres) continue;
             float cr = 0.f, ca = 0.f;
             if (d <= R) {
