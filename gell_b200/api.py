@@ -151,6 +151,14 @@ def load_library() -> ctypes.CDLL:
     L.gell_set_option.argtypes = [P, ctypes.c_int, ctypes.c_int64]
     L.gell_selftest_timeout.argtypes = [P, ctypes.c_int]
     L.gell_selftest_division.argtypes = [P, ctypes.c_int64, ctypes.c_uint64, P]
+    L.gell_surrogate_weight_count.argtypes = []
+    L.gell_surrogate_weight_count.restype = ctypes.c_longlong
+    L.gell_surrogate_load.argtypes = [P, ctypes.c_int, P, ctypes.c_longlong, ctypes.c_int, ctypes.c_float,
+                                      ctypes.c_float]
+    L.gell_lod_surrogate.argtypes = [P, ctypes.c_int, P, P]
+    L.gell_surrogate_infer.argtypes = [P, ctypes.c_int]
+    L.gell_surrogate_run_layers.argtypes = [P, ctypes.c_int, ctypes.c_int]
+    L.gell_surrogate_read.argtypes = [P, ctypes.c_int, ctypes.c_int, P, ctypes.c_longlong]
     for name in ("gell_create", "gell_destroy", "gell_set_stream", "gell_substrate_add",
                  "gell_cells_import", "gell_cells_export", "gell_cell_count", "gell_field_import",
                  "gell_field_export", "gell_fm_update", "gell_prelod", "gell_lod_solver",
@@ -162,7 +170,8 @@ def load_library() -> ctypes.CDLL:
                  "gell_save_field_slice_csv", "gell_checkpoint_save", "gell_checkpoint_load",
                  "gell_reference_spheroid", "gell_ensemble_create", "gell_ensemble_destroy",
                  "gell_ensemble_configure", "gell_ensemble_run_mechanics", "gell_ensemble_tune",
-                 "gell_ensemble_sync"):
+                 "gell_ensemble_sync", "gell_surrogate_load", "gell_lod_surrogate", "gell_surrogate_infer",
+                 "gell_surrogate_run_layers", "gell_surrogate_read"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
@@ -375,6 +384,44 @@ class Simulation:
         v = ctypes.c_int64()
         self._check(self.lib.gell_launch_count(self.h, ctypes.byref(v)), "gell_launch_count")
         return v.value
+
+    # -- learned surrogate of one substrate's LOD
+    def surrogate_load(self, sub: int, weights: np.ndarray, substeps: int = 50, rate_scale: float = 0.1,
+                       threshold: float = 1e-3) -> None:
+        """Load the operator's weights (gell_surrogate_weight_count() floats, conv3d order)."""
+        w = np.ascontiguousarray(weights, np.float32).reshape(-1)
+        self._check(self.lib.gell_surrogate_load(self.h, sub, P(w.ctypes.data), w.size, substeps, rate_scale,
+                                                 threshold), "gell_surrogate_load")
+
+    def lod_surrogate(self, sub: int) -> tuple[bool, float]:
+        """One judged surrogate step; returns (accepted, judge residual)."""
+        acc = ctypes.c_int()
+        r = ctypes.c_float()
+        self._check(self.lib.gell_lod_surrogate(self.h, sub, ctypes.byref(acc), ctypes.byref(r)),
+                    "gell_lod_surrogate")
+        return bool(acc.value), float(r.value)
+
+    def surrogate_infer(self, sub: int) -> None:
+        self._check(self.lib.gell_surrogate_infer(self.h, sub), "gell_surrogate_infer")
+
+    def surrogate_run_layers(self, sub: int, layers: int) -> None:
+        self._check(self.lib.gell_surrogate_run_layers(self.h, sub, layers), "gell_surrogate_run_layers")
+
+    def surrogate_read(self, sub: int, which: int) -> np.ndarray:
+        """which 0: input planes, 1: h, 2: t as float32 [C][N^3]; 3: the output field [N^3]."""
+        n3 = self.N ** 3
+        if which == 3:
+            P_ = (self.N + 3) // 4 * 4
+            raw = np.zeros(P_ * self.N * self.N, np.float32)
+            self._check(self.lib.gell_surrogate_read(self.h, sub, 3, P(raw.ctypes.data), raw.nbytes),
+                        "gell_surrogate_read")
+            return raw.reshape(self.N, self.N, P_)[:, :, :self.N].reshape(-1).copy()
+        planes = 2 if which == 0 else 4
+        raw = np.zeros(planes * n3 * 8, np.uint16)
+        self._check(self.lib.gell_surrogate_read(self.h, sub, which, P(raw.ctypes.data), raw.nbytes),
+                    "gell_surrogate_read")
+        f = (raw.astype(np.uint32) << 16).view(np.float32).reshape(planes, n3, 8)
+        return f.transpose(0, 2, 1).reshape(planes * 8, n3).copy()
 
     # -- parity support
     def _dump(self, what: int, arg: int, dtype, count: int) -> np.ndarray:

@@ -189,6 +189,7 @@ static void free_all(gell_ctx* c) {
     f(c->dev_epoch);
     for (auto& g : c->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
+    surrogate_free(c);
     for (auto& s : c->subs) { f(s.p); f(s.rate); f(s.EF); f(s.FRS); f(s.line_flag); f(s.line_list); f(s.line_count); }
     f(c->xorwow); f(c->flags); f(c->scan_tmp); f(c->dev_count); f(c->dev_err);
     f(c->staging);

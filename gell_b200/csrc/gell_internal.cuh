@@ -78,6 +78,8 @@ struct Geom {
     float len;    // voxel length
 };
 
+struct SurrogateState;  // learned substrate surrogate (surrogate.cu)
+
 struct SortScratch {
     uint32_t* keys[2] = {nullptr, nullptr};
     uint32_t* vals[2] = {nullptr, nullptr};
@@ -111,6 +113,7 @@ struct gell_ctx {
     bool sorted_valid = false;  // keys/perm describe the current order
 
     std::vector<gell::Substrate> subs;
+    gell::SurrogateState* sur[8] = {};  // per substrate, created by gell_surrogate_load
     bool rate_valid = false;
     bool exact_chain = false;  // GELL_OPT_EXACT_CHAIN
     int sweep_warps = 0;       // GELL_OPT_SWEEP_WARPS (0: as many as shared memory allows)
@@ -277,6 +280,7 @@ gell_status scan_u32(gell_ctx* c, const uint32_t* in, uint32_t* out, int n, int*
 // stable LSD radix sort of (keys, vals) over the low `bits` bits; result in c->sort.which
 gell_status radix_sort(gell_ctx* c, int n, int bits, bool vals_are_iota);
 gell_status dump_se(gell_ctx* c, int* host_out);
+void surrogate_free(gell_ctx* c);
 gell_status selftest_division(gell_ctx* c, long long n, unsigned long long seed, long long* mismatches);
 size_t sort_hist_entries(int cap);
 

@@ -1,0 +1,628 @@
+// surrogate.cu — learned oxygen surrogate: a 3-D convolutional operator that replaces K LOD substeps
+// of one substrate, judged after every use by one plain LOD substep and replaced by the plain solve
+// when the judge rejects it.  No reference counterpart: the reference only has the plain solver
+// (include/LODkernel.cuh:280-300), which is the fallback here and the source of the training pairs.
+//
+// Operator.  Input channels [p / b, rate * rate_scale, shell mask] (b = the substrate's boundary
+// value, shell = the four boundary layers that Setboundary rewrites), a 3x3x3 convolution to 32
+// channels with ReLU, four residual blocks h += conv(relu(conv(h))) (the inner one with ReLU), and a
+// 3x3x3 convolution to one channel d; the output field is p + b * d inside and b on the shell.  All
+// convolutions are zero-padded ("same"), weights and activations are bf16, sums are fp32.
+//
+// Activation layout in HBM ("8-channel planes").  A tensor of C channels over the N^3 voxels is
+// C/8 planes; plane q holds channels 8q..8q+7 of voxel v = x + N*(y + N*z) as 16 contiguous bytes at
+// byte 16*v.  An x-run of voxels of one plane is then exactly the canonical no-swizzle K-major
+// operand layout of the tensor cores (8 rows of 16 bytes per core matrix, consecutive voxels 16
+// bytes apart), so the operand of tap dx is the run staged for dx = 0 moved by 16*dx bytes.
+//
+// k_conv3 (implicit GEMM on tcgen05).  A tile is 128 consecutive voxels of one x-line (M = 128) by
+// all output channels (N = NOUT); K runs over the 27 taps x the input channels, 16 channels per
+// MMA.  Per tile one TMA box per (dy, dz) brings the 130-voxel run x0-1 .. x0+128 of all input
+// planes (zero fill outside the grid gives the padding), 9 boxes in all; the weights of the whole
+// layer stay in shared memory.  Warp 0 issues the TMA loads (two tile stages), one thread of warp 1
+// issues the MMAs into one of two TMEM accumulators and commits them to mbarriers, warps 2-5 read
+// the finished accumulator (tcgen05.ld), apply bias, ReLU / residual / field update and store.
+// Every wait is bounded (codes 21-27 in the context's error word).
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "async_copy.cuh"
+#include "gell_internal.cuh"
+
+namespace gell {
+
+struct SurrogateState;
+
+namespace {
+
+constexpr int kTileM = 128;                  // voxels per tile
+constexpr int kRunVox = kTileM + 2;          // staged voxels per (dy, dz) run, with the x halo
+constexpr int kRunPlaneB = kRunVox * 16;     // bytes of one plane of one staged run (2080)
+constexpr int kLayers = 10;                  // conv_in, 4 x (conv_a, conv_b), conv_out
+constexpr int kHidden = 32;
+constexpr int kInCh = 3;
+
+enum ConvMode { kRelu = 0, kResidual = 1, kField = 2 };
+
+struct ConvArgs {
+    CUtensorMap in;                 // 5-D map {8, N, N, N, planes}, box {8, 130, 1, 1, planes}
+    const uint8_t* w;               // packed weights, the shared-memory image
+    const float* bias;              // NOUT
+    uint4* out;                     // planes (kRelu, kResidual)
+    const uint4* res;               // residual planes (kResidual; may equal out)
+    float* field_out;               // pitched field (kField)
+    const float* field_in;          // pitched field (kField)
+    int N, P;
+    long long PN;
+    long long nvox;                 // N^3: plane length in voxels
+    int tiles_x;
+    long long tiles;
+    float scale, bval;              // kField: out = in + scale * d inside, bval on the shell
+    int* err;
+};
+
+// ---------------------------------------------------------------- tcgen05 / TMEM (inline PTX)
+
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t cols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
+                 "r"(cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t addr, uint32_t cols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(addr), "r"(cols) : "memory");
+}
+// Shared-memory matrix descriptor, no swizzle: start, leading-dimension byte offset (between the
+// two 8-element K chunks of an MMA), stride byte offset (between 8-row core-matrix groups), all in
+// 16-byte units; bit 46 = descriptor version of sm_100.
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// Instruction descriptor of kind::f16: fp32 accumulator, bf16 A and B, both K-major, M = 128.
+__host__ __device__ constexpr uint32_t idesc_bf16(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+__device__ __forceinline__ void mma_bf16(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc)
+        : "memory");
+}
+// The mbarrier completes one phase when every MMA issued so far by this thread has finished.
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// 32 lanes x 32 columns (x32) or 16 columns (x16) of fp32: thread t gets lane (base lane + t).
+__device__ __forceinline__ void tmem_ld32(uint32_t a, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(a));
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t a, uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(a));
+}
+
+__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* tm, int c0, int c1, int c2, int c3, int c4,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, "
+        "%6}], [%7];" ::"r"(smem_u32(dst)),
+        "l"(tm), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+    __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<uint32_t*>(&h);
+}
+__device__ __forceinline__ float2 unpack_bf16(uint32_t u) {
+    __nv_bfloat162 h = *reinterpret_cast<__nv_bfloat162*>(&u);
+    return __bfloat1622float2(h);
+}
+
+// Shared memory of one k_conv3 instance: two tile stages of 9 runs (each run padded to 128 bytes),
+// the layer's weights, ten mbarriers and the TMEM address.
+template <int CIN8, int NOUT>
+struct ConvSmem {
+    static constexpr int kRunB = (CIN8 * kRunPlaneB + 127) / 128 * 128;
+    static constexpr int kStageB = 9 * kRunB;
+    static constexpr int kHalves = CIN8 / 2;               // MMAs (16 input channels) per tap
+    static constexpr int kWBlk = NOUT * 32;                // one (tap, half) weight block
+    static constexpr int kWB = 27 * kHalves * kWBlk;
+    static constexpr int kBars = 2 * kStageB + kWB;
+    static constexpr int kBytes = kBars + 10 * 8 + 16;
+};
+
+__device__ __forceinline__ void tile_of(const ConvArgs& a, long long t, int& x0, int& y, int& z) {
+    const long long line = t / a.tiles_x;
+    x0 = (int)(t - line * a.tiles_x) * kTileM;
+    y = (int)(line % a.N);
+    z = (int)(line / a.N);
+}
+
+template <int CIN8, int NOUT, int MODE>
+__global__ void __launch_bounds__(192, 1) k_conv3(const __grid_constant__ ConvArgs a) {
+    using L = ConvSmem<CIN8, NOUT>;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t* wsm = smem + 2 * L::kStageB;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L::kBars);
+    uint64_t* full = bars;       // [2] stage loaded
+    uint64_t* empty = bars + 2;  // [2] stage consumed by the MMAs
+    uint64_t* accf = bars + 4;   // [2] accumulator complete
+    uint64_t* acce = bars + 6;   // [2] accumulator read by the epilogue (4 warps)
+    uint64_t* wbar = bars + 8;   // weights loaded
+    uint64_t* done = bars + 9;   // every MMA of this CTA finished
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 10);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+            mbar_init(&accf[i], 1);
+            mbar_init(&acce[i], 4);
+        }
+        mbar_init(wbar, 1);
+        mbar_init(done, 1);
+        fence_mbar_init();
+    }
+    if (warp == 1) tmem_alloc(tslot, 64);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const long long T = a.tiles;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            mbar_arrive_expect(wbar, (uint32_t)L::kWB);
+            for (int off = 0; off < L::kWB; off += 16384) {
+                const int nb = L::kWB - off < 16384 ? L::kWB - off : 16384;
+                bulk_load(wsm + off, a.w + off, (uint32_t)nb, wbar);
+            }
+            int k = 0;
+            for (long long t = blockIdx.x; t < T; t += gridDim.x, ++k) {
+                const int s = k & 1;
+                if (k >= 2 && !mbar_wait1(&empty[s], ((k >> 1) - 1) & 1, a.err, 21)) break;
+                int x0, y, z;
+                tile_of(a, t, x0, y, z);
+                uint8_t* st = smem + s * L::kStageB;
+                mbar_arrive_expect(&full[s], (uint32_t)(9 * CIN8 * kRunPlaneB));
+                for (int r = 0; r < 9; ++r)
+                    tma_load_5d(st + r * L::kRunB, &a.in, 0, x0 - 1, y + r % 3 - 1, z + r / 3 - 1, 0, &full[s]);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_bf16(NOUT);
+            bool ok = mbar_wait1(wbar, 0, a.err, 22);
+            const uint32_t wbase = smem_u32(wsm);
+            int k = 0;
+            for (long long t = blockIdx.x; ok && t < T; t += gridDim.x, ++k) {
+                const int s = k & 1;
+                if (!mbar_wait1(&full[s], (k >> 1) & 1, a.err, 23)) break;
+                if (k >= 2 && !mbar_wait1(&acce[s], ((k >> 1) - 1) & 1, a.err, 24)) break;
+                tc_fence_after();
+                const uint32_t d = tmem + (uint32_t)(s * 32);
+                const uint32_t sb = smem_u32(smem + s * L::kStageB);
+#pragma unroll 1
+                for (int tap = 0; tap < 27; ++tap) {
+                    const uint32_t run = sb + (uint32_t)((tap / 3) * L::kRunB + (tap % 3) * 16);
+#pragma unroll
+                    for (int h = 0; h < L::kHalves; ++h) {
+                        const uint64_t ad = sdesc(run + (uint32_t)(2 * h * kRunPlaneB), kRunPlaneB, 128);
+                        const uint64_t bd = sdesc(wbase + (uint32_t)((tap * L::kHalves + h) * L::kWBlk), NOUT * 16, 128);
+                        mma_bf16(d, ad, bd, idesc, (tap | h) != 0 ? 1u : 0u);
+                    }
+                }
+                mma_commit(&empty[s]);
+                mma_commit(&accf[s]);
+            }
+            mma_commit(done);
+            mbar_wait1(done, 0, a.err, 25);
+        }
+    } else {
+        const int q = warp & 3;  // TMEM lanes 32q..32q+31 are this warp's
+        float bias[NOUT];
+#pragma unroll
+        for (int n = 0; n < NOUT; ++n) bias[n] = a.bias[n];
+        int k = 0;
+        for (long long t = blockIdx.x; t < T; t += gridDim.x, ++k) {
+            const int s = k & 1;
+            if (!mbar_wait(&accf[s], (k >> 1) & 1, a.err, 26)) break;
+            tc_fence_after();
+            uint32_t v[NOUT];
+            const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(s * 32);
+            if constexpr (NOUT == 32) tmem_ld32(ta, v);
+            else tmem_ld16(ta, v);
+            tmem_wait_ld();
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acce[s]);
+            int x0, y, z;
+            tile_of(a, t, x0, y, z);
+            const int x = x0 + 32 * q + lane;
+            if (x >= a.N) continue;
+            if constexpr (MODE == kField) {
+                const long long pi = (long long)x + (long long)a.P * y + a.PN * z;
+                const int N = a.N;
+                const bool shell = x < 2 || x > N - 3 || y < 2 || y > N - 3 || z < 2 || z > N - 3;
+                const float d = __uint_as_float(v[0]) + bias[0];
+                a.field_out[pi] = shell ? a.bval : __fmaf_rn(a.scale, d, a.field_in[pi]);
+            } else {
+                const long long vox = (long long)x + (long long)a.N * (y + (long long)a.N * z);
+                float f[NOUT];
+#pragma unroll
+                for (int n = 0; n < NOUT; ++n) f[n] = __uint_as_float(v[n]) + bias[n];
+#pragma unroll
+                for (int pl = 0; pl < NOUT / 8; ++pl) {
+                    if constexpr (MODE == kResidual) {
+                        const uint4 r = a.res[pl * a.nvox + vox];
+                        const uint32_t rr[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            const float2 u = unpack_bf16(rr[j]);
+                            f[8 * pl + 2 * j] += u.x;
+                            f[8 * pl + 2 * j + 1] += u.y;
+                        }
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) f[8 * pl + j] = fmaxf(f[8 * pl + j], 0.f);
+                    }
+                    a.out[pl * a.nvox + vox] =
+                        make_uint4(pack_bf16(f[8 * pl], f[8 * pl + 1]), pack_bf16(f[8 * pl + 2], f[8 * pl + 3]),
+                                   pack_bf16(f[8 * pl + 4], f[8 * pl + 5]), pack_bf16(f[8 * pl + 6], f[8 * pl + 7]));
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        __syncwarp();
+        tc_fence_after();
+        tmem_dealloc(tmem, 64);
+    }
+}
+
+// Input planes of the operator: plane 0 = (p / b, rate * rate_scale, shell, 0, ...); plane 1 stays
+// zero (the first convolution reads 16 input channels).
+__global__ void k_pack_input(const float* p, const float* rate, Geom g, float inv_b, float rate_scale, uint4* out) {
+    const long long nvox = (long long)g.N * g.N * g.N;
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < nvox;
+         v += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(v % g.N);
+        const long long yz = v / g.N;
+        const int y = (int)(yz % g.N), z = (int)(yz / g.N);
+        const long long pi = x + (long long)g.P * y + g.PN * z;
+        const int N = g.N;
+        const bool shell = x < 2 || x > N - 3 || y < 2 || y > N - 3 || z < 2 || z > N - 3;
+        out[v] = make_uint4(pack_bf16(__fmul_rn(p[pi], inv_b), __fmul_rn(rate[pi], rate_scale)),
+                            pack_bf16(shell ? 1.f : 0.f, 0.f), 0u, 0u);
+    }
+}
+
+// max |a - b| over the voxels inside the shell (the values the next substep carries forward), as
+// the bits of a non-negative float (ordered like the floats).
+__global__ void k_absdiff_max(const float* a, const float* b, Geom g, unsigned* out) {
+    const int N = g.N, M = N - 4;
+    const long long n = (long long)M * M * M;
+    float m = 0.f;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(i % M) + 2;
+        const long long yz = i / M;
+        const int y = (int)(yz % M) + 2, z = (int)(yz / M) + 2;
+        const long long pi = x + (long long)g.P * y + g.PN * z;
+        m = fmaxf(m, fabsf(a[pi] - b[pi]));
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(FULL, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+}
+
+// Layer table: input planes, output channels (padded), mode.
+struct LayerShape {
+    int cin, cout, cin8, nout;
+};
+constexpr LayerShape kShape[kLayers] = {
+    {kInCh, kHidden, 2, 32},   {kHidden, kHidden, 4, 32}, {kHidden, kHidden, 4, 32}, {kHidden, kHidden, 4, 32},
+    {kHidden, kHidden, 4, 32}, {kHidden, kHidden, 4, 32}, {kHidden, kHidden, 4, 32}, {kHidden, kHidden, 4, 32},
+    {kHidden, kHidden, 4, 32}, {kHidden, 1, 4, 16}};
+
+}  // namespace
+
+// ---------------------------------------------------------------- host state
+
+struct SurrogateState {
+    int substeps = 0;
+    float rate_scale = 0.f, threshold = 0.f;
+    uint8_t* w[kLayers] = {};   // packed weight images
+    float* bias[kLayers] = {};  // padded to the layer's NOUT
+    uint4* in = nullptr;        // 2 planes
+    uint4* h = nullptr;         // 4 planes
+    uint4* t = nullptr;         // 4 planes
+    float* ph = nullptr;        // surrogate output field (pitched)
+    float* backup = nullptr;    // field before the step (pitched)
+    unsigned* dmax = nullptr;   // judge scratch
+    unsigned* hmax = nullptr;   // pinned host copy
+    CUtensorMap map_in, map_h, map_t;
+    long long conv_launches = 0;
+    double conv_flops = 0;      // algorithmic FLOPs of one inference (real channels only)
+};
+
+void surrogate_free(gell_ctx* c) {
+    for (auto*& s : c->sur) {
+        if (!s) continue;
+        for (int l = 0; l < kLayers; ++l) {
+            if (s->w[l]) cudaFree(s->w[l]);
+            if (s->bias[l]) cudaFree(s->bias[l]);
+        }
+        for (void* p : {(void*)s->in, (void*)s->h, (void*)s->t, (void*)s->ph, (void*)s->backup, (void*)s->dmax})
+            if (p) cudaFree(p);
+        if (s->hmax) cudaFreeHost(s->hmax);
+        delete s;
+        s = nullptr;
+    }
+}
+
+static gell_status plane_map(gell_ctx* c, CUtensorMap* m, void* base, int planes) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        cudaDriverEntryPointQueryResult q;
+        void* fn = nullptr;
+        cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+            return fail(c, GELL_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+        encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    const cuuint64_t N = (cuuint64_t)c->g.N;
+    const cuuint64_t dims[5] = {8, N, N, N, (cuuint64_t)planes};
+    const cuuint64_t strides[4] = {16, 16 * N, 16 * N * N, 16 * N * N * N};
+    const cuuint32_t box[5] = {8, (cuuint32_t)kRunVox, 1, 1, (cuuint32_t)planes};
+    const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    CUresult r = encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, base, dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(c, GELL_ERR_CUDA, "cuTensorMapEncodeTiled (planes) failed (" + std::to_string((int)r) + ")");
+    return GELL_OK;
+}
+
+// Pack one layer's fp32 weights W[cout][cin][3][3][3] (PyTorch conv3d order, kz kz ky kx = dz dy dx
+// + 1) into the shared-memory image: block (tap, half) holds [kc][n][8] with input channel
+// 16*half + 8*kc + e and output channel n; padding channels are zero.
+static void pack_layer(const float* W, const LayerShape& s, std::vector<uint16_t>& img) {
+    const int halves = s.cin8 / 2;
+    img.assign((size_t)27 * halves * 2 * s.nout * 8, 0);
+    auto bf = [](float f) {
+        uint32_t u;
+        std::memcpy(&u, &f, 4);
+        if ((u & 0x7fffffffu) > 0x7f800000u) return (uint16_t)0x7fc0u;
+        u += 0x7fffu + ((u >> 16) & 1u);  // round to nearest even
+        return (uint16_t)(u >> 16);
+    };
+    for (int tap = 0; tap < 27; ++tap)
+        for (int h = 0; h < halves; ++h)
+            for (int kc = 0; kc < 2; ++kc)
+                for (int n = 0; n < s.nout; ++n)
+                    for (int e = 0; e < 8; ++e) {
+                        const int ci = 16 * h + 8 * kc + e;
+                        float v = 0.f;
+                        if (n < s.cout && ci < s.cin) v = W[((size_t)n * s.cin + ci) * 27 + tap];
+                        img[((((size_t)tap * halves + h) * 2 + kc) * s.nout + n) * 8 + e] = bf(v);
+                    }
+}
+
+template <int CIN8, int NOUT, int MODE>
+static gell_status launch_conv(gell_ctx* c, SurrogateState* S, const CUtensorMap& in, int layer, uint4* out,
+                               const uint4* res, float* fout, const float* fin, float scale, float bval) {
+    using L = ConvSmem<CIN8, NOUT>;
+    // the shared-memory opt-in is a per-device attribute; setting it is cheap, so every launch does
+    GELL_CUDA(c, cudaFuncSetAttribute(k_conv3<CIN8, NOUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes));
+    ConvArgs a{};
+    a.in = in;
+    a.w = S->w[layer];
+    a.bias = S->bias[layer];
+    a.out = out;
+    a.res = res;
+    a.field_out = fout;
+    a.field_in = fin;
+    a.N = c->g.N;
+    a.P = c->g.P;
+    a.PN = c->g.PN;
+    a.nvox = c->nvox;
+    a.tiles_x = (c->g.N + kTileM - 1) / kTileM;
+    a.tiles = (long long)a.tiles_x * c->g.N * c->g.N;
+    a.scale = scale;
+    a.bval = bval;
+    a.err = c->dev_err;
+    int sms = 0;
+    GELL_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+    const int grid = (int)(a.tiles < sms ? a.tiles : sms);
+    GELL_KERNEL(c, "k_conv3", (k_conv3<CIN8, NOUT, MODE><<<grid, 192, L::kBytes, c->stream>>>(a)));
+    S->conv_launches++;
+    return GELL_OK;
+}
+
+// The input packing and the first `layers` convolutions of one inference of substrate `sub`:
+//   layer 0        h  = relu(conv_in(input))
+//   layer 2k+1     t  = relu(conv_a(h))          (k = 0..3)
+//   layer 2k+2     h += conv_b(t)
+//   layer 9        S->ph = p + b * conv_out(h) inside the shell, b on it
+static gell_status run_layers(gell_ctx* c, int sub, SurrogateState* S, int layers) {
+    Substrate& Su = c->subs[sub];
+    const float b = Su.s.boundary;
+    const int pb = blocks_for(c->nvox, 256);
+    GELL_KERNEL(c, "k_pack_input",
+                (k_pack_input<<<pb < 148 * 16 ? pb : 148 * 16, 256, 0, c->stream>>>(Su.p, Su.rate, c->g, 1.f / b,
+                                                                                 S->rate_scale, S->in)));
+    gell_status st = GELL_OK;
+    for (int l = 0; l < layers && st == GELL_OK; ++l) {
+        if (l == 0) st = launch_conv<2, 32, kRelu>(c, S, S->map_in, 0, S->h, nullptr, nullptr, nullptr, 0.f, 0.f);
+        else if (l == kLayers - 1) st = launch_conv<4, 16, kField>(c, S, S->map_h, l, nullptr, nullptr, S->ph, Su.p, b, b);
+        else if (l & 1) st = launch_conv<4, 32, kRelu>(c, S, S->map_h, l, S->t, nullptr, nullptr, nullptr, 0.f, 0.f);
+        else st = launch_conv<4, 32, kResidual>(c, S, S->map_t, l, S->h, S->h, nullptr, nullptr, 0.f, 0.f);
+    }
+    return st;
+}
+static gell_status infer(gell_ctx* c, int sub, SurrogateState* S) { return run_layers(c, sub, S, kLayers); }
+
+}  // namespace gell
+
+using namespace gell;
+
+static long long weight_count() {
+    long long n = 0;
+    for (const auto& s : kShape) n += (long long)s.cout * s.cin * 27 + s.cout;
+    return n;
+}
+
+extern "C" {
+
+long long gell_surrogate_weight_count(void) { return weight_count(); }
+
+gell_status gell_surrogate_load(gell_ctx* c, int sub, const float* weights, long long count, int substeps,
+                                float rate_scale, float threshold) {
+    GELL_RANGE("gell_surrogate_load");
+    if (!c || !weights || sub < 0 || sub >= (int)c->subs.size() || substeps < 1) return GELL_ERR_INVALID_ARG;
+    if (count != weight_count()) return fail(c, GELL_ERR_INVALID_ARG, "surrogate weight count does not match the operator");
+    if (!(c->subs[sub].s.boundary != 0.f)) return fail(c, GELL_ERR_UNSUPPORTED, "the surrogate scales by the boundary value, which is 0");
+    if (c->g.N < 8 || c->g.N > 1023) return fail(c, GELL_ERR_UNSUPPORTED, "grid edge outside the surrogate's range");
+    SurrogateState* S = c->sur[sub];  // reloading keeps the buffers and replaces the weights
+    const bool fresh = S == nullptr;
+    if (fresh) S = new SurrogateState();
+    S->substeps = substeps;
+    S->rate_scale = rate_scale;
+    S->threshold = threshold;
+    S->conv_flops = 0;
+    const float* W = weights;
+    for (int l = 0; l < kLayers; ++l) {
+        const LayerShape& s = kShape[l];
+        std::vector<uint16_t> img;
+        pack_layer(W, s, img);
+        W += (size_t)s.cout * s.cin * 27;
+        std::vector<float> bias(s.nout, 0.f);
+        for (int n = 0; n < s.cout; ++n) bias[n] = W[n];
+        W += s.cout;
+        S->conv_flops += 2.0 * (double)c->nvox * s.cout * s.cin * 27;
+        if (!S->w[l]) {
+            c->sur[sub] = S;  // owned by the context from here on (freed with it)
+            if (cudaMalloc(&S->w[l], img.size() * 2) != cudaSuccess || cudaMalloc(&S->bias[l], bias.size() * 4) != cudaSuccess)
+                return fail(c, GELL_ERR_ALLOC, "surrogate weights");
+        }
+        GELL_CUDA(c, cudaMemcpy(S->w[l], img.data(), img.size() * 2, cudaMemcpyHostToDevice));
+        GELL_CUDA(c, cudaMemcpy(S->bias[l], bias.data(), bias.size() * 4, cudaMemcpyHostToDevice));
+    }
+    c->sur[sub] = S;
+    if (fresh) {
+        const size_t plane = (size_t)c->nvox * 16, field = (size_t)c->nvox_p * 4;
+        if (cudaMalloc(&S->in, 2 * plane) != cudaSuccess || cudaMalloc(&S->h, 4 * plane) != cudaSuccess ||
+            cudaMalloc(&S->t, 4 * plane) != cudaSuccess || cudaMalloc(&S->ph, field) != cudaSuccess ||
+            cudaMalloc(&S->backup, field) != cudaSuccess || cudaMalloc(&S->dmax, 4) != cudaSuccess ||
+            cudaMallocHost(&S->hmax, 4) != cudaSuccess)
+            return fail(c, GELL_ERR_ALLOC, "surrogate activations (10 planes of 16 bytes per voxel)");
+        GELL_CUDA(c, cudaMemset(S->in, 0, 2 * plane));
+        gell_status st = plane_map(c, &S->map_in, S->in, 2);
+        if (st == GELL_OK) st = plane_map(c, &S->map_h, S->h, 4);
+        if (st == GELL_OK) st = plane_map(c, &S->map_t, S->t, 4);
+        if (st != GELL_OK) return st;
+    }
+    return GELL_OK;
+}
+
+gell_status gell_surrogate_infer(gell_ctx* c, int sub) {
+    GELL_RANGE("gell_surrogate_infer");
+    if (!c || sub < 0 || sub >= (int)c->subs.size()) return GELL_ERR_INVALID_ARG;
+    SurrogateState* S = c->sur[sub];
+    if (!S) return fail(c, GELL_ERR_INVALID_ARG, "no surrogate loaded for this substrate");
+    gell_status st = infer(c, sub, S);
+    if (st != GELL_OK) return st;
+    GELL_CUDA(c, cudaMemcpyAsync(c->subs[sub].p, S->ph, (size_t)c->nvox_p * 4, cudaMemcpyDeviceToDevice, c->stream));
+    return GELL_OK;
+}
+
+gell_status gell_lod_surrogate(gell_ctx* c, int sub, int* accepted, float* residual) {
+    GELL_RANGE("gell_lod_surrogate");
+    if (!c || sub < 0 || sub >= (int)c->subs.size()) return GELL_ERR_INVALID_ARG;
+    SurrogateState* S = c->sur[sub];
+    if (!S) return fail(c, GELL_ERR_INVALID_ARG, "no surrogate loaded for this substrate");
+    Substrate& Su = c->subs[sub];
+    const size_t fb = (size_t)c->nvox_p * 4;
+    GELL_CUDA(c, cudaMemcpyAsync(S->backup, Su.p, fb, cudaMemcpyDeviceToDevice, c->stream));
+    gell_status st = infer(c, sub, S);
+    if (st != GELL_OK) return st;
+    // judge: one plain substep from the surrogate's field; a field on the solver's trajectory moves
+    // little in one substep
+    GELL_CUDA(c, cudaMemcpyAsync(Su.p, S->ph, fb, cudaMemcpyDeviceToDevice, c->stream));
+    st = lod_solver(c, sub, 1);
+    if (st != GELL_OK) return st;
+    GELL_CUDA(c, cudaMemsetAsync(S->dmax, 0, 4, c->stream));
+    GELL_KERNEL(c, "k_absdiff_max", (k_absdiff_max<<<148 * 8, 256, 0, c->stream>>>(Su.p, S->ph, c->g, S->dmax)));
+    GELL_CUDA(c, cudaMemcpyAsync(S->hmax, S->dmax, 4, cudaMemcpyDeviceToHost, c->stream));
+    GELL_CUDA(c, cudaStreamSynchronize(c->stream));
+    float r;
+    std::memcpy(&r, S->hmax, 4);
+    r /= Su.s.boundary;
+    if (residual) *residual = r;
+    const bool ok = r <= S->threshold;
+    if (accepted) *accepted = ok ? 1 : 0;
+    if (ok) {
+        GELL_CUDA(c, cudaMemcpyAsync(Su.p, S->ph, fb, cudaMemcpyDeviceToDevice, c->stream));
+        return GELL_OK;
+    }
+    GELL_CUDA(c, cudaMemcpyAsync(Su.p, S->backup, fb, cudaMemcpyDeviceToDevice, c->stream));
+    return lod_solver(c, sub, S->substeps);
+}
+
+gell_status gell_surrogate_run_layers(gell_ctx* c, int sub, int layers) {
+    if (!c || sub < 0 || sub >= (int)c->subs.size() || layers < 0 || layers > kLayers) return GELL_ERR_INVALID_ARG;
+    SurrogateState* S = c->sur[sub];
+    if (!S) return fail(c, GELL_ERR_INVALID_ARG, "no surrogate loaded for this substrate");
+    return run_layers(c, sub, S, layers);
+}
+
+gell_status gell_surrogate_read(gell_ctx* c, int sub, int which, void* host, long long bytes) {
+    if (!c || !host || sub < 0 || sub >= (int)c->subs.size() || !c->sur[sub]) return GELL_ERR_INVALID_ARG;
+    SurrogateState* S = c->sur[sub];
+    const long long plane = c->nvox * 16;
+    const void* src = which == 0 ? (const void*)S->in : which == 1 ? (const void*)S->h : which == 2 ? (const void*)S->t
+                    : which == 3 ? (const void*)S->ph : nullptr;
+    const long long need = which == 0 ? 2 * plane : which == 3 ? c->nvox_p * 4 : 4 * plane;
+    if (!src || bytes != need) return GELL_ERR_INVALID_ARG;
+    GELL_CUDA(c, cudaMemcpyAsync(host, src, (size_t)bytes, cudaMemcpyDeviceToHost, c->stream));
+    GELL_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GELL_OK;
+}
+
+}  // extern "C"

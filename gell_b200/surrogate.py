@@ -1,0 +1,250 @@
+"""The learned LOD surrogate: weight files, the operator as a PyTorch module (for fitting), training
+pairs from the plain solver, and the judge's calibration.
+
+The operator itself runs in the library (gell_surrogate_load / gell_lod_surrogate, hand-written
+tcgen05 convolutions); this module only produces its weights.  Training pairs come from the plain
+LOD solver (the reference's LODsolver, include/LODkernel.cuh:280-300, bit-exact in this library):
+input (p, uptake map, shell) -> p after `substeps` substeps, over seeded jittered-lattice
+spheroids with the large plain-method workload's statistics (volume fraction 0.6, radii N(5, 0.5)
+um) placed at random centres with seeded Ki-67 states, each followed for several blocks of
+substeps from the boundary value, so that the pairs run from transient fields to quasi-steady ones.
+
+Weight file: 8-byte magic b"GSUR0001", int32 substeps, float32 rate_scale, float32 threshold,
+int64 count, then `count` float32 weights in gell_surrogate_load's order (little-endian).
+"""
+from __future__ import annotations
+
+import struct
+from dataclasses import dataclass
+
+import numpy as np
+
+MAGIC = b"GSUR0001"
+SHAPES = [(3, 32)] + [(32, 32)] * 8 + [(32, 1)]  # (cin, cout) of the ten convolutions
+
+
+@dataclass
+class SurrogateWeights:
+    weights: np.ndarray
+    substeps: int = 50
+    rate_scale: float = 0.1
+    threshold: float = 1e-3
+
+
+def save_weights(path: str, sw: SurrogateWeights) -> None:
+    w = np.ascontiguousarray(sw.weights, np.float32).reshape(-1)
+    with open(path, "wb") as f:
+        f.write(MAGIC)
+        f.write(struct.pack("<iffq", sw.substeps, sw.rate_scale, sw.threshold, w.size))
+        f.write(w.astype("<f4").tobytes())
+
+
+def load_weights(path: str) -> SurrogateWeights:
+    with open(path, "rb") as f:
+        if f.read(8) != MAGIC:
+            raise ValueError(f"{path}: not a surrogate weight file")
+        substeps, rate_scale, threshold, n = struct.unpack("<iffq", f.read(20))
+        w = np.frombuffer(f.read(4 * n), "<f4").astype(np.float32)
+    if w.size != n:
+        raise ValueError(f"{path}: truncated")
+    return SurrogateWeights(w, substeps, rate_scale, threshold)
+
+
+def weight_count() -> int:
+    return sum(co * ci * 27 + co for ci, co in SHAPES)
+
+
+def shell_mask(N: int) -> np.ndarray:
+    """The four boundary layers of every face (Setboundary, include/LODkernel.cuh:112-136)."""
+    g = np.arange(N)
+    s = (g < 2) | (g > N - 3)
+    return (s[:, None, None] | s[None, :, None] | s[None, None, :]).ravel()
+
+
+def make_torch_operator():
+    """The operator as a torch.nn.Module with the library's layer order and semantics."""
+    import torch
+    from torch import nn
+
+    class Operator(nn.Module):
+        def __init__(self):
+            super().__init__()
+            self.convs = nn.ModuleList(nn.Conv3d(ci, co, 3, padding=1) for ci, co in SHAPES)
+            nn.init.zeros_(self.convs[-1].weight)  # starts as the identity map p -> p
+            nn.init.zeros_(self.convs[-1].bias)
+
+        def forward(self, x, p, b, shell):
+            h = torch.relu(self.convs[0](x))
+            for k in range(4):
+                t = torch.relu(self.convs[1 + 2 * k](h))
+                h = h + self.convs[2 + 2 * k](t)
+            d = self.convs[9](h)[:, 0]
+            return torch.where(shell, torch.full_like(p, b), p + b * d)
+
+        def flat_weights(self) -> np.ndarray:
+            parts = []
+            for c in self.convs:
+                parts.append(c.weight.detach().float().cpu().numpy().ravel())
+                parts.append(c.bias.detach().float().cpu().numpy().ravel())
+            return np.concatenate(parts).astype(np.float32)
+
+    return Operator()
+
+
+class PairSource:
+    """Training or validation pairs from a few contexts, each following one spheroid for
+    `blocks` blocks of `substeps` plain substeps before the next spheroid replaces it."""
+
+    def __init__(self, N: int, cells: tuple[int, int], seed: int, substeps: int = 50, blocks: int = 10,
+                 contexts: int = 4, length: float = 10.0):
+        import gell_b200 as gb
+        self.gb, self.N, self.cells, self.substeps, self.blocks, self.length = gb, N, cells, substeps, blocks, length
+        self.rng = np.random.Generator(np.random.Philox(seed))
+        self.sims = []
+        self.left = []
+        for _ in range(contexts):
+            sim = gb.Simulation(voxel_num=N, voxel_length=length, max_cell_num=cells[1])
+            sim.add_substrate(gb.oxygen())
+            self.sims.append(sim)
+            self.left.append(0)
+        self.k = 0
+
+    def _reseed(self, sim) -> None:
+        gb, N, L = self.gb, self.N, self.N * self.length
+        n = int(np.exp(self.rng.uniform(np.log(self.cells[0]), np.log(self.cells[1]))))
+        a = (4.0 / 3.0 * np.pi * 125.0 / 0.6) ** (1.0 / 3.0)
+        r = a * (3.0 * n / (4.0 * np.pi)) ** (1.0 / 3.0)
+        lo, hi = r + 4 * self.length, L - r - 4 * self.length
+        centre = self.rng.uniform(lo, hi, 3) if hi > lo else np.full(3, L / 2)
+        c = gb.lattice_spheroid(n, centre, int(self.rng.integers(1 << 30)), self.length, N)
+        c = gb.seed_ki67_states(c, int(self.rng.integers(1 << 30)))
+        sim.import_cells(c)
+        sim.set_field(0, np.full(N ** 3, sim_boundary(gb), np.float32))
+        sim.PreLOD()
+
+    def next(self):
+        """(p, rate, target) as float32 arrays of N^3 values."""
+        i = self.k % len(self.sims)
+        self.k += 1
+        sim = self.sims[i]
+        if self.left[i] == 0:
+            self._reseed(sim)
+            self.left[i] = self.blocks
+        # a random number of extra substeps spreads the pairs over the trajectory
+        extra = int(self.rng.integers(0, self.substeps))
+        if extra:
+            sim.LODsolver(extra, 0)
+        p = sim.field(0)
+        rate = sim.dump_rate(0)
+        sim.LODsolver(self.substeps, 0)
+        self.left[i] -= 1
+        return p, rate, sim.field(0)
+
+    def close(self) -> None:
+        for s in self.sims:
+            s.close()
+
+
+def sim_boundary(gb) -> float:
+    return float(gb.oxygen().boundary)
+
+
+def train(N: int = 256, pairs: int = 2000, substeps: int = 50, rate_scale: float = 0.1, seed: int = 11,
+          cells: tuple[int, int] = (150_000, 450_000), lr: float = 1e-3, log=print) -> SurrogateWeights:
+    """Fit the operator on `pairs` pairs (one per iteration, never reused) with Adam on the mean
+    squared error inside the shell, in units of the boundary value."""
+    import torch
+    import gell_b200 as gb
+
+    dev = torch.device("cuda")
+    b = sim_boundary(gb)
+    net = make_torch_operator().to(dev)
+    opt = torch.optim.Adam(net.parameters(), lr=lr)
+    sched = torch.optim.lr_scheduler.CosineAnnealingLR(opt, pairs)
+    shell = torch.from_numpy(shell_mask(N)).to(dev).reshape(1, N, N, N)
+    inner = ~shell
+    src = PairSource(N, cells, seed, substeps)
+    try:
+        for it in range(pairs):
+            p, rate, tgt = src.next()
+            pt = torch.from_numpy(p).to(dev).reshape(1, N, N, N)
+            x = torch.stack([pt / b, torch.from_numpy(rate).to(dev).reshape(1, N, N, N) * rate_scale,
+                             shell.float()], 1)
+            y = torch.from_numpy(tgt).to(dev).reshape(1, N, N, N)
+            with torch.autocast("cuda", dtype=torch.bfloat16):
+                q = net(x, pt, b, shell)
+            err = ((q.float() - y) / b)[inner]
+            loss = (err * err).mean()
+            opt.zero_grad(set_to_none=True)
+            loss.backward()
+            opt.step()
+            sched.step()
+            if it % 100 == 0 or it == pairs - 1:
+                log(f"pair {it}: rmse {loss.sqrt().item():.3e} linf {err.abs().max().item():.3e}")
+    finally:
+        src.close()
+    return SurrogateWeights(net.flat_weights(), substeps, rate_scale, 0.0)
+
+
+def calibrate(sw: SurrogateWeights, N: int = 256, pairs: int = 64, seed: int = 1234,
+              cells: tuple[int, int] = (150_000, 450_000), tol: float = 0.01, log=print):
+    """Run the library's operator and judge on held-out pairs and set the threshold: the judge's
+    residual r bounds the error e (L-infinity inside the shell, units of the boundary value) on
+    these pairs as e <= kappa * r with kappa the largest ratio seen; threshold = tol / kappa.
+    Returns (threshold, [(r, e)])."""
+    import gell_b200 as gb
+
+    src = PairSource(N, cells, seed, sw.substeps)
+    b = sim_boundary(gb)
+    inner = ~shell_mask(N)
+    out = []
+    try:
+        with gb.Simulation(voxel_num=N, voxel_length=10.0, max_cell_num=cells[1]) as sim:
+            sim.add_substrate(gb.oxygen())
+            sim.surrogate_load(0, sw.weights, sw.substeps, sw.rate_scale, 1e30)
+            for _ in range(pairs):
+                i = src.k % len(src.sims)
+                p, rate, tgt = src.next()
+                # the same state in the judging context: cells of the source context
+                sim.import_cells(src.sims[i].export_cells())
+                sim.PreLOD()
+                sim.set_field(0, p)
+                _, r = sim.lod_surrogate(0)
+                q = sim.field(0)
+                e = float(np.abs(q - tgt)[inner].max() / b)
+                out.append((r, e))
+    finally:
+        src.close()
+    kappa = max(e / max(r, 1e-12) for r, e in out)
+    thr = tol / kappa
+    log(f"calibration: kappa {kappa:.3g}, threshold {thr:.3e}, accepted {sum(r <= thr for r, _ in out)}/{len(out)}")
+    return thr, out
+
+
+def main(argv=None) -> int:
+    import argparse
+    import time
+
+    ap = argparse.ArgumentParser(description="Fit the LOD surrogate of oxygen and calibrate its judge.")
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--N", type=int, default=256)
+    ap.add_argument("--pairs", type=int, default=2000)
+    ap.add_argument("--val-pairs", type=int, default=64)
+    ap.add_argument("--substeps", type=int, default=50)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--tol", type=float, default=0.01)
+    a = ap.parse_args(argv)
+    t0 = time.time()
+    sw = train(a.N, a.pairs, a.substeps, lr=a.lr)
+    t1 = time.time()
+    print(f"fit: {a.pairs} pairs in {t1 - t0:.1f} s", flush=True)
+    sw.threshold, pts = calibrate(sw, a.N, a.val_pairs, tol=a.tol)
+    print(f"calibration: {a.val_pairs} pairs in {time.time() - t1:.1f} s", flush=True)
+    for r, e in pts:
+        print(f"  r {r:.3e}  e {e:.3e}")
+    save_weights(a.out, sw)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -337,6 +337,37 @@ gell_status gell_ensemble_tune(gell_ensemble* ens, int substeps, int* steps_take
                                int* best_sweep_warps);
 gell_status gell_ensemble_sync(gell_ensemble* ens);
 
+/* Learned surrogate of one substrate's LOD (no reference counterpart; the reference's plain solver,
+ * LODsolver in include/LODkernel.cuh:280-300, is its fallback and the source of its training pairs).
+ * A 3-D convolutional operator maps [p / b, uptake rate * rate_scale, boundary-shell mask] to the
+ * field after `substeps` LOD substeps: conv 3->32 + ReLU, four residual blocks
+ * h += conv(ReLU(conv(h))), conv 32->1 giving d; output p + b * d inside the four boundary layers
+ * and b on them (b = the substrate's boundary value).  3x3x3 kernels, zero padding, bf16 weights and
+ * activations, fp32 sums, hand-written tcgen05 kernels.
+ *
+ * gell_surrogate_load: `weights` holds gell_surrogate_weight_count() floats, layer by layer
+ * (conv_in, conv_a/conv_b of blocks 1-4, conv_out), each the PyTorch conv3d weight
+ * [cout][cin][3][3][3] followed by its bias [cout].  Allocates the operator's buffers (40 bytes per
+ * voxel of bf16 activations, two fields) on the first load; a later load replaces the weights.
+ * gell_lod_surrogate: one judged step of `substeps` LOD substeps of the substrate (the uptake map
+ * must be current, as for gell_lod_solver).  The operator's field q is judged by one plain substep
+ * L: r = max |L(q) - q| / b over the voxels inside the boundary layers.  r <= threshold keeps q
+ * (*accepted = 1); otherwise the field is restored and the plain solver runs the substeps
+ * (*accepted = 0).  Synchronises the stream once (the decision is taken on the host).
+ * gell_surrogate_infer: the operator alone, field := q (no judge).
+ * gell_surrogate_run_layers / gell_surrogate_read: the input packing and the first `layers` (0..10)
+ * convolutions, and a copy of a buffer to the host (which: 0 = input planes, 2 x 16 bytes per voxel;
+ * 1 = h, 2 = t, 4 x 16 bytes per voxel; 3 = the output field, pitched) — for tests.  Activations are
+ * stored as planes of 8 channels: plane q holds channels 8q..8q+7 of voxel x + N*(y + N*z) as 8
+ * bf16 values at byte 16*(voxel + q*N^3). */
+long long gell_surrogate_weight_count(void);
+gell_status gell_surrogate_load(gell_ctx* ctx, int substrate, const float* weights, long long count, int substeps,
+                                float rate_scale, float threshold);
+gell_status gell_lod_surrogate(gell_ctx* ctx, int substrate, int* accepted, float* residual);
+gell_status gell_surrogate_infer(gell_ctx* ctx, int substrate);
+gell_status gell_surrogate_run_layers(gell_ctx* ctx, int substrate, int layers);
+gell_status gell_surrogate_read(gell_ctx* ctx, int substrate, int which, void* host, long long bytes);
+
 /* Number of kernels this context has launched (always counted). */
 gell_status gell_launch_count(gell_ctx* ctx, int64_t* count);
 

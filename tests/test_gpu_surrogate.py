@@ -1,0 +1,143 @@
+"""The learned LOD surrogate on the GPU: its tcgen05 convolutions against PyTorch fp32 convolutions of
+the same bf16 operands, and the judge / fallback contract against the plain solver.
+
+Each layer is checked on its own input as the CUDA path stored it (bf16 planes read back through
+the C ABI), so rounding does not compound: the stored output must equal the fp32 reference rounded
+to bf16 within one bf16 unit (2^-8 relative; the two sums differ only in order).  The output
+field (fp32) must match within 1e-5 of the boundary value.
+"""
+import numpy as np
+import pytest
+
+from cases import ball_cells, random_field
+
+pytestmark = pytest.mark.gpu
+
+gb = pytest.importorskip("gell_b200")
+torch = pytest.importorskip("torch")
+
+SHAPES = [(3, 32)] + [(32, 32)] * 8 + [(32, 1)]
+
+
+def random_weights(seed, scale=1.0):
+    rng = np.random.Generator(np.random.Philox(seed))
+    out = []
+    for cin, cout in SHAPES:
+        std = scale / np.sqrt(cin * 27)
+        out.append(rng.normal(0, std, (cout, cin, 3, 3, 3)).astype(np.float32).ravel())
+        out.append(rng.normal(0, 0.1, cout).astype(np.float32))
+    w = np.concatenate(out)
+    assert w.size == gb.load_library().gell_surrogate_weight_count()
+    return w
+
+
+def layer_params(w):
+    """[(W[cout,cin,3,3,3], b[cout])] with W rounded to bf16 as the kernels store it."""
+    out, i = [], 0
+    for cin, cout in SHAPES:
+        n = cout * cin * 27
+        W = torch.from_numpy(w[i:i + n].reshape(cout, cin, 3, 3, 3)).to(torch.bfloat16).float()
+        i += n
+        b = torch.from_numpy(w[i:i + cout].copy())
+        i += cout
+        out.append((W.cuda(), b.cuda()))
+    return out
+
+
+def conv(x, Wb, N):
+    W, b = Wb
+    xt = torch.from_numpy(x).cuda().reshape(1, x.shape[0], N, N, N)  # [C][z][y][x]
+    return torch.nn.functional.conv3d(xt, W, b, padding=1)[0].reshape(W.shape[0], -1).cpu().numpy()
+
+
+def assert_bf16_close(got, ref, what):
+    tol = np.abs(ref) * 2.0 ** -8 + 1e-6
+    bad = np.abs(got - ref) > tol
+    assert not bad.any(), (what, int(bad.sum()), float(np.abs(got - ref).max()))
+
+
+def make_sim(N, seed, cells=2000):
+    sim = gb.Simulation(voxel_num=N, voxel_length=10.0, max_cell_num=max(cells, 16))
+    sim.add_substrate(gb.oxygen())
+    sim.import_cells(ball_cells(N, 10.0, cells, seed, dead_frac=0.0, outside=0))
+    sim.set_field(0, random_field(N, seed, 20.0, 38.0))
+    sim.PreLOD()
+    return sim
+
+
+@pytest.mark.parametrize("N", [40, 136])
+def test_surrogate_layers_match_torch(N):
+    w = random_weights(3)
+    Ws = layer_params(w)
+    with make_sim(N, 5) as sim:
+        sim.surrogate_load(0, w, 50, 0.1, 1.0)
+        b = 38.0
+        sim.surrogate_run_layers(0, 0)
+        x = sim.surrogate_read(0, 0)[:3]
+        # input planes: p / b, rate * 0.1, shell
+        p = sim.field(0)
+        rate = sim.dump_rate(0)
+        bf = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(torch.bfloat16).float().numpy()
+        assert np.array_equal(x[0], bf(p * np.float32(1.0 / b)))
+        assert np.array_equal(x[1], bf(rate * np.float32(0.1)))
+        g = np.arange(N)
+        sh = (g < 2) | (g > N - 3)
+        shell = (sh[:, None, None] | sh[None, :, None] | sh[None, None, :]).ravel()
+        assert np.array_equal(x[2], shell.astype(np.float32))
+        prev_h = None
+        for l in range(10):
+            sim.surrogate_run_layers(0, l)
+            h_in, t_in = sim.surrogate_read(0, 1), sim.surrogate_read(0, 2)
+            sim.surrogate_run_layers(0, l + 1)
+            if l == 0:
+                ref = np.maximum(conv(x, Ws[0], N), 0)
+                assert_bf16_close(sim.surrogate_read(0, 1), ref, "layer 0")
+            elif l == 9:
+                d = conv(h_in, Ws[9], N)[0]
+                ref = np.where(shell, np.float32(b), p + np.float32(b) * d)
+                got = sim.surrogate_read(0, 3)
+                assert np.abs(got - ref).max() <= 1e-5 * b, np.abs(got - ref).max()
+            elif l % 2 == 1:
+                ref = np.maximum(conv(h_in, Ws[l], N), 0)
+                assert_bf16_close(sim.surrogate_read(0, 2), ref, f"layer {l}")
+            else:
+                ref = h_in + conv(t_in, Ws[l], N)
+                assert_bf16_close(sim.surrogate_read(0, 1), ref, f"layer {l}")
+            prev_h = h_in
+        assert prev_h is not None
+        assert sim.launch_count() > 0
+        sim.sync()
+
+
+def test_judge_accepts_and_falls_back():
+    N, K = 48, 50
+    w = random_weights(4)
+    # conv_out all zero: the operator returns p inside and b on the shell
+    n_out = 32 * 27 + 1
+    w[-n_out:] = 0
+    with make_sim(N, 6, 3000) as a, make_sim(N, 6, 3000) as ref:
+        a.surrogate_load(0, w, K, 0.1, 1e9)
+        p0 = a.field(0)
+        ok, r = a.lod_surrogate(0)
+        assert ok and r > 0
+        q = a.field(0)
+        g = np.arange(N)
+        sh = (g < 2) | (g > N - 3)
+        shell = (sh[:, None, None] | sh[None, :, None] | sh[None, None, :]).ravel()
+        assert np.array_equal(q[~shell], p0[~shell]) and np.all(q[shell] == np.float32(38.0))
+        # the judge residual is one plain substep's change of that field
+        a.set_field(0, q)
+        a.LODsolver(1, 0)
+        l1 = a.field(0)
+        inner = np.zeros((N, N, N), bool)
+        inner[2:N - 2, 2:N - 2, 2:N - 2] = True
+        inner = inner.ravel()
+        assert np.float32(np.abs(l1 - q)[inner].max() / np.float32(38.0)) == np.float32(r)
+        # a threshold below every residual: the field is exactly the plain solver's K substeps
+        a.set_field(0, p0)
+        a.surrogate_load(0, w, K, 0.1, -1.0)
+        ok, r2 = a.lod_surrogate(0)
+        assert not ok and r2 == r
+        ref.LODsolver(K, 0)
+        assert np.array_equal(a.field(0).view(np.uint32), ref.field(0).view(np.uint32))
+        a.sync()
