@@ -433,6 +433,131 @@ def c4_members(gb, stream):
     return sims, edges
 
 
+# ---------------------------------------------------------------------------- surrogate workload
+
+C5_N, C5_CELLS, C5_WARM = 256, 300_000, 1000
+C5_WORKLOAD = ("learned surrogate (pattern 4): 256^3 grid of 10 um, oxygen, 300,000 cells (seeded jittered-lattice "
+               "spheroid with the large workload's statistics and seeded Ki-67 states); one block = FM_update + PreLOD "
+               "+ K = 50 LOD substeps, the substeps either plain or replaced by the judged 3-D conv operator "
+               "(4 residual blocks, 32 channels, 3^3 kernels, bf16 operands, fp32 sums) from the same state")
+C5_WEIGHTS = os.path.join(ROOT, "gell_b200", "data", "o2_surrogate_256.gsur")
+
+
+def bf16_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured bf16_tflops (cuBLAS burst)"
+    except Exception:
+        return 1590.0, "fallback"
+
+
+def run_c5(args, rank, world, local_rank):
+    """--workload c5: blocks of a quasi-steady spheroid; per block the same state is advanced by the
+    plain solver and by the judged surrogate, each timed with CUDA events on the context's stream;
+    the simulation continues from the judged result, as a surrogate-driven run would."""
+    import torch
+    import gell_b200 as gb
+    from gell_b200 import surrogate as gs
+
+    torch.cuda.set_device(local_rank)
+    sw = gs.load_weights(args.surrogate_weights or C5_WEIGHTS)
+    K = sw.substeps
+    cells = gb.lattice_spheroid(C5_CELLS, C5_N * LENGTH / 2, 5, LENGTH, C5_N)
+    gb.seed_ki67_states(cells, 13)
+    sim = gb.Simulation(voxel_num=C5_N, voxel_length=LENGTH, max_cell_num=C5_CELLS)
+    sim.add_substrate(gb.oxygen())
+    stream = torch.cuda.Stream()
+    sim.set_stream(stream)
+    sim.import_cells(cells)
+    sim.PreLOD()
+    sim.LODsolver(C5_WARM, 0)  # from the boundary value to a quasi-steady field
+    sim.set_conv_ring(not args.no_conv_ring)
+    sim.surrogate_load(0, sw.weights, K, sw.rate_scale, sw.threshold)
+    b = float(gb.oxygen().boundary)
+    inner = ~gs.shell_mask(C5_N)
+    for _ in range(args.warmup):  # untimed: kernels loaded, buffers touched
+        sim.FM_update()
+        sim.PreLOD()
+        p = sim.field(0)
+        sim.lod_surrogate(0)
+        sim.set_field(0, p)
+        sim.LODsolver(K, 0)
+    sim.sync()
+
+    props = torch.cuda.get_device_properties(local_rank)
+    uuid = getattr(props, "uuid", None)
+    uuid = f"GPU-{uuid}" if uuid is not None and not str(uuid).startswith("GPU-") else uuid
+    sampler = ClockSampler(str(uuid) if uuid else None)
+    sampler.start()
+    time.sleep(0.3)
+    t_plain, t_sur, errs, res, acc = [], [], [], [], []
+    for _ in range(args.steps):
+        sim.FM_update()
+        sim.PreLOD()
+        p = sim.field(0)
+        e0, e1, e2, e3 = (torch.cuda.Event(enable_timing=True) for _ in range(4))
+        torch.cuda.synchronize()
+        e0.record(stream)
+        sim.LODsolver(K, 0)
+        e1.record(stream)
+        ref = sim.field(0)
+        sim.set_field(0, p)
+        torch.cuda.synchronize()
+        e2.record(stream)
+        ok, r = sim.lod_surrogate(0)
+        e3.record(stream)
+        q = sim.field(0)
+        t_plain.append(e0.elapsed_time(e1))
+        t_sur.append(e2.elapsed_time(e3))
+        errs.append(float(np.abs(q - ref)[inner].max() / b))
+        res.append(r)
+        acc.append(ok)
+    sampler.stop()
+    # operator kernels alone, from the per-kernel event profile of a few inferences
+    sim.profile(True)
+    sim.profile_read(reset=True)
+    p = sim.field(0)
+    for _ in range(3):
+        sim.surrogate_infer(0)
+        sim.set_field(0, p)
+    prof = sim.profile_read(reset=True)
+    sim.profile(False)
+    sim.close()
+    tp, ts = float(np.mean(t_plain)), float(np.mean(t_sur))
+    hid = prof.get("k_conv3_hidden", (0, 0.0))
+    infer_ms = sum(v[1] for k, v in prof.items() if k.startswith("k_conv3") or k == "k_pack_input") / 3
+    flops_hidden = 2.0 * C5_N ** 3 * 32 * 32 * 27
+    peak, peak_src = bf16_peak()
+    avg_hidden = hid[1] / max(hid[0], 1)
+    achieved = flops_hidden / (avg_hidden / 1e3) / 1e12 if hid[0] else None
+    acc_errs = [e for e, a in zip(errs, acc) if a]
+    line = {
+        "metric": "oxygen LOD substeps/s with the judged surrogate (256^3, 300k cells)",
+        "value": K / (ts / 1e3), "unit": "substeps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ts, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
+        "data": "synthetic: seeded jittered-lattice spheroid of 300,000 cells; weights fitted on 2,000 pairs from the "
+                "plain solver (gell_b200.surrogate)",
+        "config": {"workload": C5_WORKLOAD, "voxels": C5_N ** 3, "substeps_per_block": K,
+                   "conv_ring": not args.no_conv_ring,
+                   "warm_substeps": C5_WARM, "judge_threshold": sw.threshold, "l2": "each field is 67 MB; the "
+                   "operator's activations are 1.07 GB per 32-channel tensor"},
+        "plain": {"value": K / (tp / 1e3), "ms_per_block": tp},
+        "speedup_vs_plain": tp / ts,
+        "accuracy": {"linf_err_max": max(errs), "linf_err_max_accepted": max(acc_errs) if acc_errs else None,
+                     "linf_err_mean": float(np.mean(errs)), "accepted": int(sum(acc)), "blocks": len(acc),
+                     "judge_residual_max": max(res), "unit": "max |q - p_plain| / boundary value inside the shell"},
+        "components": {"ms_inference": infer_ms, "ms_conv_hidden_per_launch": avg_hidden,
+                       "kernels": {k: [v[0] / 3, v[1] / 3] for k, v in prof.items()}},
+        "roofline": {"kernel": "k_conv3_hidden (32 -> 32, 256^3)", "bound": "tensor", "achieved": achieved,
+                     "peak": peak, "peak_source": peak_src, "unit": "TFLOP/s",
+                     "frac": achieved / peak if achieved else None, "traffic": None,
+                     "flops_per_launch": flops_hidden},
+        "gpu_launches": None, "clocks": sampler.summary(),
+    }
+    return line
+
+
 def run_c4(args, rank, world, local_rank):
     """--workload c4: K mechanics steps of all members in biology periods of 60."""
     import torch
@@ -598,9 +723,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("gell", "reference"), default="gell")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=("large", "c3", "c4"), default="large",
+    ap.add_argument("--workload", choices=("large", "c3", "c4", "c5"), default="large",
                     help="large: 400^3, 10^6 cells (the headline line); c3: 600^3, 5*10^6 cells with "
-                         "birth/death; c4: ensemble of 64 small instances")
+                         "birth/death; c4: ensemble of 64 small instances; c5: the learned oxygen surrogate "
+                         "against the plain solver at 256^3")
+    ap.add_argument("--surrogate-weights", default=None, help="c5: weight file (default: the packaged one)")
+    ap.add_argument("--no-conv-ring", action="store_true", help="c5: convolutions without the row ring")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -620,8 +748,8 @@ def main():
         import torch.distributed as td
         torch.cuda.set_device(local_rank)
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    if args.workload in ("c3", "c4"):
-        line = (run_c3 if args.workload == "c3" else run_c4)(args, rank, world, local_rank)
+    if args.workload in ("c3", "c4", "c5"):
+        line = {"c3": run_c3, "c4": run_c4, "c5": run_c5}[args.workload](args, rank, world, local_rank)
         if rank == 0:
             print(json.dumps(line), flush=True)
         if world > 1:

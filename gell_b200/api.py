@@ -380,6 +380,10 @@ class Simulation:
         """Run every LOD back-substitution group on the exact division chain (same results)."""
         self._check(self.lib.gell_set_option(self.h, 1, int(bool(on))), "gell_set_option")
 
+    def set_conv_ring(self, on: bool = True) -> None:
+        """The surrogate's convolutions with (default) or without the row ring along y."""
+        self._check(self.lib.gell_set_option(self.h, 4, int(bool(on))), "gell_set_option")
+
     def launch_count(self) -> int:
         v = ctypes.c_int64()
         self._check(self.lib.gell_launch_count(self.h, ctypes.byref(v)), "gell_launch_count")

@@ -172,6 +172,45 @@ __device__ __forceinline__ void tile_of(const ConvArgs& a, long long t, int& x0,
     z = (int)(line / a.N);
 }
 
+// Epilogue of one accumulator row (voxel x of line (y, z)): bias, then ReLU, residual add or the
+// field update, and the store.
+template <int NOUT, int MODE>
+__device__ __forceinline__ void store_tile(const ConvArgs& a, const uint32_t (&v)[NOUT], const float (&bias)[NOUT],
+                                           int x, int y, int z) {
+    if (x >= a.N) return;
+    if constexpr (MODE == kField) {
+        const long long pi = (long long)x + (long long)a.P * y + a.PN * z;
+        const int N = a.N;
+        const bool shell = x < 2 || x > N - 3 || y < 2 || y > N - 3 || z < 2 || z > N - 3;
+        const float d = __uint_as_float(v[0]) + bias[0];
+        a.field_out[pi] = shell ? a.bval : __fmaf_rn(a.scale, d, a.field_in[pi]);
+    } else {
+        const long long vox = (long long)x + (long long)a.N * (y + (long long)a.N * z);
+        float f[NOUT];
+#pragma unroll
+        for (int n = 0; n < NOUT; ++n) f[n] = __uint_as_float(v[n]) + bias[n];
+#pragma unroll
+        for (int pl = 0; pl < NOUT / 8; ++pl) {
+            if constexpr (MODE == kResidual) {
+                const uint4 r = a.res[pl * a.nvox + vox];
+                const uint32_t rr[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const float2 u = unpack_bf16(rr[j]);
+                    f[8 * pl + 2 * j] += u.x;
+                    f[8 * pl + 2 * j + 1] += u.y;
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) f[8 * pl + j] = fmaxf(f[8 * pl + j], 0.f);
+            }
+            a.out[pl * a.nvox + vox] =
+                make_uint4(pack_bf16(f[8 * pl], f[8 * pl + 1]), pack_bf16(f[8 * pl + 2], f[8 * pl + 3]),
+                           pack_bf16(f[8 * pl + 4], f[8 * pl + 5]), pack_bf16(f[8 * pl + 6], f[8 * pl + 7]));
+        }
+    }
+}
+
 template <int CIN8, int NOUT, int MODE>
 __global__ void __launch_bounds__(192, 1) k_conv3(const __grid_constant__ ConvArgs a) {
     using L = ConvSmem<CIN8, NOUT>;
@@ -228,7 +267,7 @@ __global__ void __launch_bounds__(192, 1) k_conv3(const __grid_constant__ ConvAr
         if (lane == 0) {
             constexpr uint32_t idesc = idesc_bf16(NOUT);
             bool ok = mbar_wait1(wbar, 0, a.err, 22);
-            const uint32_t wbase = smem_u32(wsm);
+            const uint64_t b0 = sdesc(smem_u32(wsm), NOUT * 16, 128);
             int k = 0;
             for (long long t = blockIdx.x; ok && t < T; t += gridDim.x, ++k) {
                 const int s = k & 1;
@@ -236,15 +275,16 @@ __global__ void __launch_bounds__(192, 1) k_conv3(const __grid_constant__ ConvAr
                 if (k >= 2 && !mbar_wait1(&acce[s], ((k >> 1) - 1) & 1, a.err, 24)) break;
                 tc_fence_after();
                 const uint32_t d = tmem + (uint32_t)(s * 32);
-                const uint32_t sb = smem_u32(smem + s * L::kStageB);
-#pragma unroll 1
+                const uint64_t a0 = sdesc(smem_u32(smem + s * L::kStageB), kRunPlaneB, 128);
+                // descriptors differ only in the start address (low 14 bits, 16-byte units, no carry
+                // out: shared memory is below 256 KB), so each MMA adds a compile-time offset
+#pragma unroll
                 for (int tap = 0; tap < 27; ++tap) {
-                    const uint32_t run = sb + (uint32_t)((tap / 3) * L::kRunB + (tap % 3) * 16);
 #pragma unroll
                     for (int h = 0; h < L::kHalves; ++h) {
-                        const uint64_t ad = sdesc(run + (uint32_t)(2 * h * kRunPlaneB), kRunPlaneB, 128);
-                        const uint64_t bd = sdesc(wbase + (uint32_t)((tap * L::kHalves + h) * L::kWBlk), NOUT * 16, 128);
-                        mma_bf16(d, ad, bd, idesc, (tap | h) != 0 ? 1u : 0u);
+                        const uint32_t ao = ((tap / 3) * L::kRunB + (tap % 3) * 16 + 2 * h * kRunPlaneB) >> 4;
+                        const uint32_t bo = ((tap * L::kHalves + h) * L::kWBlk) >> 4;
+                        mma_bf16(d, a0 + ao, b0 + bo, idesc, (tap | h) != 0 ? 1u : 0u);
                     }
                 }
                 mma_commit(&empty[s]);
@@ -273,38 +313,182 @@ __global__ void __launch_bounds__(192, 1) k_conv3(const __grid_constant__ ConvAr
             if (lane == 0) mbar_arrive(&acce[s]);
             int x0, y, z;
             tile_of(a, t, x0, y, z);
-            const int x = x0 + 32 * q + lane;
-            if (x >= a.N) continue;
-            if constexpr (MODE == kField) {
-                const long long pi = (long long)x + (long long)a.P * y + a.PN * z;
-                const int N = a.N;
-                const bool shell = x < 2 || x > N - 3 || y < 2 || y > N - 3 || z < 2 || z > N - 3;
-                const float d = __uint_as_float(v[0]) + bias[0];
-                a.field_out[pi] = shell ? a.bval : __fmaf_rn(a.scale, d, a.field_in[pi]);
-            } else {
-                const long long vox = (long long)x + (long long)a.N * (y + (long long)a.N * z);
-                float f[NOUT];
-#pragma unroll
-                for (int n = 0; n < NOUT; ++n) f[n] = __uint_as_float(v[n]) + bias[n];
-#pragma unroll
-                for (int pl = 0; pl < NOUT / 8; ++pl) {
-                    if constexpr (MODE == kResidual) {
-                        const uint4 r = a.res[pl * a.nvox + vox];
-                        const uint32_t rr[4] = {r.x, r.y, r.z, r.w};
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            const float2 u = unpack_bf16(rr[j]);
-                            f[8 * pl + 2 * j] += u.x;
-                            f[8 * pl + 2 * j + 1] += u.y;
-                        }
-                    } else {
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) f[8 * pl + j] = fmaxf(f[8 * pl + j], 0.f);
+            store_tile<NOUT, MODE>(a, v, bias, x0 + 32 * q + lane, y, z);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        __syncwarp();
+        tc_fence_after();
+        tmem_dealloc(tmem, 64);
+    }
+}
+
+// ---------------------------------------------------------------- k_conv3_ring
+// The same convolution with the input rows reused along y.  Work comes in units of up to kUnitY
+// consecutive lines y0..y1-1 at one (x tile, z); a unit needs the row groups y0-1 .. y1 (a group =
+// the three runs z-1, z, z+1 at one y, all planes), each loaded once into a ring of kRing group
+// slots and used by the (up to) three tiles y-1, y, y+1 whose taps reach it.  A group's slot is
+// released (tcgen05.commit on its empty barrier) by the last tile that reads it: the oldest group
+// of every tile but the unit's last, and all three groups of the last.  L2 -> shared traffic is
+// one group (3 runs) per tile instead of three.
+constexpr int kUnitY = 32;
+constexpr int kRing = 6;
+
+template <int CIN8, int NOUT>
+struct RingSmem {
+    static constexpr int kRunB = (CIN8 * kRunPlaneB + 127) / 128 * 128;
+    static constexpr int kGroupB = 3 * kRunB;
+    static constexpr int kHalves = CIN8 / 2;
+    static constexpr int kWBlk = NOUT * 32;
+    static constexpr int kWB = 27 * kHalves * kWBlk;
+    static constexpr int kBars = kRing * kGroupB + kWB;
+    static constexpr int kBytes = kBars + (2 * kRing + 6) * 8 + 16;
+};
+
+__device__ __forceinline__ void unit_of(const ConvArgs& a, long long u, int& x0, int& y0, int& y1, int& z) {
+    const int nyc = (a.N + kUnitY - 1) / kUnitY;
+    const long long r = u / a.tiles_x;
+    x0 = (int)(u - r * a.tiles_x) * kTileM;
+    y0 = (int)(r % nyc) * kUnitY;
+    y1 = y0 + kUnitY < a.N ? y0 + kUnitY : a.N;
+    z = (int)(r / nyc);
+}
+
+template <int CIN8, int NOUT, int MODE>
+__global__ void __launch_bounds__(192, 1) k_conv3_ring(const __grid_constant__ ConvArgs a) {
+    using L = RingSmem<CIN8, NOUT>;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t* wsm = smem + kRing * L::kGroupB;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L::kBars);
+    uint64_t* full = bars;               // [kRing] group loaded
+    uint64_t* empty = bars + kRing;      // [kRing] group released by the MMAs
+    uint64_t* accf = bars + 2 * kRing;   // [2]
+    uint64_t* acce = accf + 2;           // [2] (4 epilogue warps)
+    uint64_t* wbar = acce + 2;
+    uint64_t* done = wbar + 1;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kRing; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+        }
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&accf[i], 1);
+            mbar_init(&acce[i], 4);
+        }
+        mbar_init(wbar, 1);
+        mbar_init(done, 1);
+        fence_mbar_init();
+    }
+    if (warp == 1) tmem_alloc(tslot, 64);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const int nyc = (a.N + kUnitY - 1) / kUnitY;
+    const long long U = (long long)a.tiles_x * nyc * a.N;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            mbar_arrive_expect(wbar, (uint32_t)L::kWB);
+            for (int off = 0; off < L::kWB; off += 16384) {
+                const int nb = L::kWB - off < 16384 ? L::kWB - off : 16384;
+                bulk_load(wsm + off, a.w + off, (uint32_t)nb, wbar);
+            }
+            bool ok = true;
+            int g = 0;
+            for (long long u = blockIdx.x; ok && u < U; u += gridDim.x) {
+                int x0, y0, y1, z;
+                unit_of(a, u, x0, y0, y1, z);
+                for (int yy = y0 - 1; yy <= y1; ++yy, ++g) {
+                    const int sl = g % kRing;
+                    if (g >= kRing && !mbar_wait1(&empty[sl], ((g / kRing) - 1) & 1, a.err, 21)) {
+                        ok = false;
+                        break;
                     }
-                    a.out[pl * a.nvox + vox] =
-                        make_uint4(pack_bf16(f[8 * pl], f[8 * pl + 1]), pack_bf16(f[8 * pl + 2], f[8 * pl + 3]),
-                                   pack_bf16(f[8 * pl + 4], f[8 * pl + 5]), pack_bf16(f[8 * pl + 6], f[8 * pl + 7]));
+                    uint8_t* gb = smem + sl * L::kGroupB;
+                    mbar_arrive_expect(&full[sl], (uint32_t)(3 * CIN8 * kRunPlaneB));
+                    for (int dz = 0; dz < 3; ++dz)
+                        tma_load_5d(gb + dz * L::kRunB, &a.in, 0, x0 - 1, yy, z + dz - 1, 0, &full[sl]);
                 }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_bf16(NOUT);
+            bool ok = mbar_wait1(wbar, 0, a.err, 22);
+            const uint64_t b0 = sdesc(smem_u32(wsm), NOUT * 16, 128);
+            const uint32_t rbase = smem_u32(smem);
+            int g = 0, k = 0;
+            for (long long u = blockIdx.x; ok && u < U; u += gridDim.x) {
+                int x0, y0, y1, z;
+                unit_of(a, u, x0, y0, y1, z);
+                const int ny = y1 - y0;
+                for (int i = 0; i < ny; ++i, ++k) {
+                    const int ac = k & 1;
+                    for (int j = 0; j < 3 && ok; ++j) {
+                        const int gg = g + i + j;
+                        ok = mbar_wait1(&full[gg % kRing], (gg / kRing) & 1, a.err, 23);
+                    }
+                    if (ok && k >= 2) ok = mbar_wait1(&acce[ac], ((k >> 1) - 1) & 1, a.err, 24);
+                    if (!ok) break;
+                    tc_fence_after();
+                    const uint32_t d = tmem + (uint32_t)(ac * 32);
+                    uint64_t ga[3];  // descriptors of the three row groups (start addresses differ)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j)
+                        ga[j] = sdesc(rbase + (uint32_t)(((g + i + j) % kRing) * L::kGroupB), kRunPlaneB, 128);
+#pragma unroll
+                    for (int tap = 0; tap < 27; ++tap) {
+#pragma unroll
+                        for (int h = 0; h < L::kHalves; ++h) {
+                            const uint32_t ao = ((tap / 9) * L::kRunB + (tap % 3) * 16 + 2 * h * kRunPlaneB) >> 4;
+                            const uint32_t bo = ((tap * L::kHalves + h) * L::kWBlk) >> 4;
+                            mma_bf16(d, ga[(tap / 3) % 3] + ao, b0 + bo, idesc, (tap | h) != 0 ? 1u : 0u);
+                        }
+                    }
+                    mma_commit(&accf[ac]);
+                    if (i < ny - 1) {
+                        mma_commit(&empty[(g + i) % kRing]);
+                    } else {
+                        for (int j = 0; j < 3; ++j) mma_commit(&empty[(g + i + j) % kRing]);
+                    }
+                }
+                g += ny + 2;
+            }
+            mma_commit(done);
+            mbar_wait1(done, 0, a.err, 25);
+        }
+    } else {
+        const int q = warp & 3;
+        float bias[NOUT];
+#pragma unroll
+        for (int n = 0; n < NOUT; ++n) bias[n] = a.bias[n];
+        int k = 0;
+        bool ok = true;
+        for (long long u = blockIdx.x; ok && u < U; u += gridDim.x) {
+            int x0, y0, y1, z;
+            unit_of(a, u, x0, y0, y1, z);
+            for (int y = y0; y < y1; ++y, ++k) {
+                const int ac = k & 1;
+                if (!mbar_wait(&accf[ac], (k >> 1) & 1, a.err, 26)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                uint32_t v[NOUT];
+                const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(ac * 32);
+                if constexpr (NOUT == 32) tmem_ld32(ta, v);
+                else tmem_ld16(ta, v);
+                tmem_wait_ld();
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&acce[ac]);
+                store_tile<NOUT, MODE>(a, v, bias, x0 + 32 * q + lane, y, z);
             }
         }
     }
@@ -445,11 +629,17 @@ static void pack_layer(const float* W, const LayerShape& s, std::vector<uint16_t
 }
 
 template <int CIN8, int NOUT, int MODE>
-static gell_status launch_conv(gell_ctx* c, SurrogateState* S, const CUtensorMap& in, int layer, uint4* out,
+static gell_status launch_conv(gell_ctx* c, const char* name, SurrogateState* S, const CUtensorMap& in, int layer, uint4* out,
                                const uint4* res, float* fout, const float* fin, float scale, float bval) {
     using L = ConvSmem<CIN8, NOUT>;
+    using R = RingSmem<CIN8, NOUT>;
     // the shared-memory opt-in is a per-device attribute; setting it is cheap, so every launch does
-    GELL_CUDA(c, cudaFuncSetAttribute(k_conv3<CIN8, NOUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes));
+    if (c->conv_ring)
+        GELL_CUDA(c, cudaFuncSetAttribute(k_conv3_ring<CIN8, NOUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          R::kBytes));
+    else
+        GELL_CUDA(c, cudaFuncSetAttribute(k_conv3<CIN8, NOUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          L::kBytes));
     ConvArgs a{};
     a.in = in;
     a.w = S->w[layer];
@@ -469,8 +659,14 @@ static gell_status launch_conv(gell_ctx* c, SurrogateState* S, const CUtensorMap
     a.err = c->dev_err;
     int sms = 0;
     GELL_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-    const int grid = (int)(a.tiles < sms ? a.tiles : sms);
-    GELL_KERNEL(c, "k_conv3", (k_conv3<CIN8, NOUT, MODE><<<grid, 192, L::kBytes, c->stream>>>(a)));
+    if (c->conv_ring) {
+        const long long units = (long long)a.tiles_x * ((c->g.N + kUnitY - 1) / kUnitY) * c->g.N;
+        const int grid = (int)(units < sms ? units : sms);
+        GELL_KERNEL(c, name, (k_conv3_ring<CIN8, NOUT, MODE><<<grid, 192, R::kBytes, c->stream>>>(a)));
+    } else {
+        const int grid = (int)(a.tiles < sms ? a.tiles : sms);
+        GELL_KERNEL(c, name, (k_conv3<CIN8, NOUT, MODE><<<grid, 192, L::kBytes, c->stream>>>(a)));
+    }
     S->conv_launches++;
     return GELL_OK;
 }
@@ -489,10 +685,10 @@ static gell_status run_layers(gell_ctx* c, int sub, SurrogateState* S, int layer
                                                                                  S->rate_scale, S->in)));
     gell_status st = GELL_OK;
     for (int l = 0; l < layers && st == GELL_OK; ++l) {
-        if (l == 0) st = launch_conv<2, 32, kRelu>(c, S, S->map_in, 0, S->h, nullptr, nullptr, nullptr, 0.f, 0.f);
-        else if (l == kLayers - 1) st = launch_conv<4, 16, kField>(c, S, S->map_h, l, nullptr, nullptr, S->ph, Su.p, b, b);
-        else if (l & 1) st = launch_conv<4, 32, kRelu>(c, S, S->map_h, l, S->t, nullptr, nullptr, nullptr, 0.f, 0.f);
-        else st = launch_conv<4, 32, kResidual>(c, S, S->map_t, l, S->h, S->h, nullptr, nullptr, 0.f, 0.f);
+        if (l == 0) st = launch_conv<2, 32, kRelu>(c, "k_conv3_in", S, S->map_in, 0, S->h, nullptr, nullptr, nullptr, 0.f, 0.f);
+        else if (l == kLayers - 1) st = launch_conv<4, 16, kField>(c, "k_conv3_out", S, S->map_h, l, nullptr, nullptr, S->ph, Su.p, b, b);
+        else if (l & 1) st = launch_conv<4, 32, kRelu>(c, "k_conv3_hidden", S, S->map_h, l, S->t, nullptr, nullptr, nullptr, 0.f, 0.f);
+        else st = launch_conv<4, 32, kResidual>(c, "k_conv3_hidden", S, S->map_t, l, S->h, S->h, nullptr, nullptr, 0.f, 0.f);
     }
     return st;
 }

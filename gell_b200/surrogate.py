@@ -6,8 +6,11 @@ tcgen05 convolutions); this module only produces its weights.  Training pairs co
 LOD solver (the reference's LODsolver, include/LODkernel.cuh:280-300, bit-exact in this library):
 input (p, uptake map, shell) -> p after `substeps` substeps, over seeded jittered-lattice
 spheroids with the large plain-method workload's statistics (volume fraction 0.6, radii N(5, 0.5)
-um) placed at random centres with seeded Ki-67 states, each followed for several blocks of
-substeps from the boundary value, so that the pairs run from transient fields to quasi-steady ones.
+um) placed at random centres with seeded Ki-67 states.  The surrogate stands in for the substeps of
+a quasi-steady field between mechanics steps, so each spheroid's field is first relaxed from the
+boundary value by a few hundred plain substeps, and each pair is one block of the running model:
+a few mechanics steps (FM_update) move the cells, PreLOD rebuilds the uptake map, and the field
+before and after `substeps` plain substeps form the pair.
 
 Weight file: 8-byte magic b"GSUR0001", int32 substeps, float32 rate_scale, float32 threshold,
 int64 count, then `count` float32 weights in gell_surrogate_load's order (little-endian).
@@ -20,6 +23,8 @@ from dataclasses import dataclass
 import numpy as np
 
 MAGIC = b"GSUR0001"
+# weights fitted for oxygen (the large workload's parameters) on 256^3 grids of 10 um
+DEFAULT_WEIGHTS = __import__("os").path.join(__import__("os").path.dirname(__file__), "data", "o2_surrogate_256.gsur")
 SHAPES = [(3, 32)] + [(32, 32)] * 8 + [(32, 1)]  # (cin, cout) of the ten convolutions
 
 
@@ -92,13 +97,17 @@ def make_torch_operator():
 
 
 class PairSource:
-    """Training or validation pairs from a few contexts, each following one spheroid for
-    `blocks` blocks of `substeps` plain substeps before the next spheroid replaces it."""
+    """Training or validation pairs from a few contexts, each following one spheroid for `blocks`
+    blocks before the next spheroid replaces it.  A new spheroid's field is relaxed by a number of
+    plain substeps drawn from `warm`; every block moves the cells by a number of mechanics steps
+    drawn from `moves`."""
 
-    def __init__(self, N: int, cells: tuple[int, int], seed: int, substeps: int = 50, blocks: int = 10,
-                 contexts: int = 4, length: float = 10.0):
+    def __init__(self, N: int, cells: tuple[int, int], seed: int, substeps: int = 50, blocks: int = 8,
+                 contexts: int = 4, length: float = 10.0, warm: tuple[int, int] = (300, 1000),
+                 moves: tuple[int, int] = (1, 5)):
         import gell_b200 as gb
         self.gb, self.N, self.cells, self.substeps, self.blocks, self.length = gb, N, cells, substeps, blocks, length
+        self.warm, self.moves = warm, moves
         self.rng = np.random.Generator(np.random.Philox(seed))
         self.sims = []
         self.left = []
@@ -121,6 +130,7 @@ class PairSource:
         sim.import_cells(c)
         sim.set_field(0, np.full(N ** 3, sim_boundary(gb), np.float32))
         sim.PreLOD()
+        sim.LODsolver(int(self.rng.integers(self.warm[0], self.warm[1] + 1)), 0)
 
     def next(self):
         """(p, rate, target) as float32 arrays of N^3 values."""
@@ -130,10 +140,9 @@ class PairSource:
         if self.left[i] == 0:
             self._reseed(sim)
             self.left[i] = self.blocks
-        # a random number of extra substeps spreads the pairs over the trajectory
-        extra = int(self.rng.integers(0, self.substeps))
-        if extra:
-            sim.LODsolver(extra, 0)
+        for _ in range(int(self.rng.integers(self.moves[0], self.moves[1] + 1))):
+            sim.FM_update()
+        sim.PreLOD()
         p = sim.field(0)
         rate = sim.dump_rate(0)
         sim.LODsolver(self.substeps, 0)
@@ -150,15 +159,20 @@ def sim_boundary(gb) -> float:
 
 
 def train(N: int = 256, pairs: int = 2000, substeps: int = 50, rate_scale: float = 0.1, seed: int = 11,
-          cells: tuple[int, int] = (150_000, 450_000), lr: float = 1e-3, log=print) -> SurrogateWeights:
-    """Fit the operator on `pairs` pairs (one per iteration, never reused) with Adam on the mean
-    squared error inside the shell, in units of the boundary value."""
+          cells: tuple[int, int] = (150_000, 450_000), lr: float = 3e-4, max_seconds: float = float("inf"),
+          log=print) -> SurrogateWeights:
+    """Fit the operator on `pairs` pairs (one per iteration, never reused) with Adam (gradient norm
+    clipped at 1, cosine decay) on the mean squared error inside the shell, in units of the boundary
+    value; stops early after `max_seconds`.  The log compares with the identity map q = p."""
+    import time
     import torch
     import gell_b200 as gb
 
     dev = torch.device("cuda")
     b = sim_boundary(gb)
-    net = make_torch_operator().to(dev)
+    t0 = time.time()
+    cl = torch.channels_last_3d
+    net = make_torch_operator().to(dev).to(memory_format=cl)
     opt = torch.optim.Adam(net.parameters(), lr=lr)
     sched = torch.optim.lr_scheduler.CosineAnnealingLR(opt, pairs)
     shell = torch.from_numpy(shell_mask(N)).to(dev).reshape(1, N, N, N)
@@ -169,7 +183,7 @@ def train(N: int = 256, pairs: int = 2000, substeps: int = 50, rate_scale: float
             p, rate, tgt = src.next()
             pt = torch.from_numpy(p).to(dev).reshape(1, N, N, N)
             x = torch.stack([pt / b, torch.from_numpy(rate).to(dev).reshape(1, N, N, N) * rate_scale,
-                             shell.float()], 1)
+                             shell.float()], 1).contiguous(memory_format=cl)
             y = torch.from_numpy(tgt).to(dev).reshape(1, N, N, N)
             with torch.autocast("cuda", dtype=torch.bfloat16):
                 q = net(x, pt, b, shell)
@@ -177,10 +191,16 @@ def train(N: int = 256, pairs: int = 2000, substeps: int = 50, rate_scale: float
             loss = (err * err).mean()
             opt.zero_grad(set_to_none=True)
             loss.backward()
+            torch.nn.utils.clip_grad_norm_(net.parameters(), 1.0)
             opt.step()
             sched.step()
-            if it % 100 == 0 or it == pairs - 1:
-                log(f"pair {it}: rmse {loss.sqrt().item():.3e} linf {err.abs().max().item():.3e}")
+            if it % 50 == 0 or it == pairs - 1:
+                ident = ((pt - y) / b)[inner].abs().max().item()
+                log(f"pair {it} ({time.time() - t0:.0f} s): rmse {loss.sqrt().item():.3e} "
+                    f"linf {err.abs().max().item():.3e} (identity linf {ident:.3e})")
+            if time.time() - t0 > max_seconds:
+                log(f"stopped after {it + 1} pairs ({max_seconds:.0f} s)")
+                break
     finally:
         src.close()
     return SurrogateWeights(net.flat_weights(), substeps, rate_scale, 0.0)
@@ -213,6 +233,7 @@ def calibrate(sw: SurrogateWeights, N: int = 256, pairs: int = 64, seed: int = 1
                 q = sim.field(0)
                 e = float(np.abs(q - tgt)[inner].max() / b)
                 out.append((r, e))
+                log(f"  r {r:.3e}  e {e:.3e}  identity {float(np.abs(p - tgt)[inner].max() / b):.3e}")
     finally:
         src.close()
     kappa = max(e / max(r, 1e-12) for r, e in out)
@@ -231,17 +252,17 @@ def main(argv=None) -> int:
     ap.add_argument("--pairs", type=int, default=2000)
     ap.add_argument("--val-pairs", type=int, default=64)
     ap.add_argument("--substeps", type=int, default=50)
-    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--lr", type=float, default=3e-4)
     ap.add_argument("--tol", type=float, default=0.01)
+    ap.add_argument("--max-seconds", type=float, default=float("inf"))
     a = ap.parse_args(argv)
     t0 = time.time()
-    sw = train(a.N, a.pairs, a.substeps, lr=a.lr)
+    sw = train(a.N, a.pairs, a.substeps, lr=a.lr, max_seconds=a.max_seconds,
+               log=lambda m: print(m, flush=True))
     t1 = time.time()
     print(f"fit: {a.pairs} pairs in {t1 - t0:.1f} s", flush=True)
-    sw.threshold, pts = calibrate(sw, a.N, a.val_pairs, tol=a.tol)
+    sw.threshold, pts = calibrate(sw, a.N, a.val_pairs, tol=a.tol, log=lambda m: print(m, flush=True))
     print(f"calibration: {a.val_pairs} pairs in {time.time() - t1:.1f} s", flush=True)
-    for r, e in pts:
-        print(f"  r {r:.3e}  e {e:.3e}")
     save_weights(a.out, sw)
     return 0
 
