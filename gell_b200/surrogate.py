@@ -242,11 +242,53 @@ def calibrate(sw: SurrogateWeights, N: int = 256, pairs: int = 64, seed: int = 1
     return thr, out
 
 
+def time_inference(N: int = 128, reps: int = 3, ring: bool = True, path: str | None = None, cells: int = 40_000,
+                   log=print) -> dict:
+    """Per-kernel device times of `reps` inferences of the operator on an N^3 grid holding a
+    quasi-steady spheroid of `cells` cells (CUDA events per launch, the library's profiler)."""
+    import gell_b200 as gb
+
+    sw = load_weights(path or DEFAULT_WEIGHTS)
+    c = gb.lattice_spheroid(cells, N * 10.0 / 2, 5, 10.0, N)
+    with gb.Simulation(voxel_num=N, voxel_length=10.0, max_cell_num=cells) as sim:
+        sim.add_substrate(gb.oxygen())
+        sim.import_cells(c)
+        sim.PreLOD()
+        sim.LODsolver(100, 0)
+        sim.set_conv_ring(ring)
+        sim.surrogate_load(0, sw.weights, sw.substeps, sw.rate_scale, sw.threshold)
+        sim.surrogate_infer(0)  # first launches (module loading) outside the timing
+        sim.profile(True)
+        sim.profile_read(reset=True)
+        for _ in range(reps):
+            sim.surrogate_infer(0)
+        prof = sim.profile_read(reset=True)
+    out = {k: {"launches": v[0] / reps, "ms_per_inference": v[1] / reps, "ms_per_launch": v[1] / v[0]}
+           for k, v in prof.items()}
+    log(out)
+    return out
+
+
 def main(argv=None) -> int:
     import argparse
+    import sys
     import time
 
-    ap = argparse.ArgumentParser(description="Fit the LOD surrogate of oxygen and calibrate its judge.")
+    argv = sys.argv[1:] if argv is None else argv
+    if argv and argv[0] == "time":
+        tp = argparse.ArgumentParser(description="Time the operator's kernels on an N^3 grid.")
+        tp.add_argument("--N", type=int, default=128)
+        tp.add_argument("--reps", type=int, default=3)
+        tp.add_argument("--no-ring", action="store_true")
+        tp.add_argument("--weights", default=None)
+        t = tp.parse_args(argv[1:])
+        time_inference(t.N, t.reps, not t.no_ring, t.weights)
+        return 0
+    if argv and argv[0] == "fit":
+        argv = argv[1:]
+    ap = argparse.ArgumentParser(description="Fit the LOD surrogate of oxygen and calibrate its judge "
+                                             "(`python -m gell_b200.surrogate [fit] --out FILE`; "
+                                             "`... time --N 128` times the operator's kernels).")
     ap.add_argument("--out", required=True)
     ap.add_argument("--N", type=int, default=256)
     ap.add_argument("--pairs", type=int, default=2000)
