@@ -159,6 +159,9 @@ def load_library() -> ctypes.CDLL:
     L.gell_surrogate_infer.argtypes = [P, ctypes.c_int]
     L.gell_surrogate_run_layers.argtypes = [P, ctypes.c_int, ctypes.c_int]
     L.gell_surrogate_read.argtypes = [P, ctypes.c_int, ctypes.c_int, P, ctypes.c_longlong]
+    L.gell_surrogate_train_init.argtypes = [P, ctypes.c_int, P, ctypes.c_longlong, ctypes.c_int, ctypes.c_float]
+    L.gell_surrogate_train_pair.argtypes = [P, ctypes.c_int, ctypes.c_float, P]
+    L.gell_surrogate_train_read.argtypes = [P, ctypes.c_int, ctypes.c_int, P, ctypes.c_longlong]
     for name in ("gell_create", "gell_destroy", "gell_set_stream", "gell_substrate_add",
                  "gell_cells_import", "gell_cells_export", "gell_cell_count", "gell_field_import",
                  "gell_field_export", "gell_fm_update", "gell_prelod", "gell_lod_solver",
@@ -171,7 +174,8 @@ def load_library() -> ctypes.CDLL:
                  "gell_reference_spheroid", "gell_ensemble_create", "gell_ensemble_destroy",
                  "gell_ensemble_configure", "gell_ensemble_run_mechanics", "gell_ensemble_tune",
                  "gell_ensemble_sync", "gell_surrogate_load", "gell_lod_surrogate", "gell_surrogate_infer",
-                 "gell_surrogate_run_layers", "gell_surrogate_read"):
+                 "gell_surrogate_run_layers", "gell_surrogate_read", "gell_surrogate_train_init",
+                 "gell_surrogate_train_pair", "gell_surrogate_train_read"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
@@ -426,6 +430,31 @@ class Simulation:
                     "gell_surrogate_read")
         f = (raw.astype(np.uint32) << 16).view(np.float32).reshape(planes, n3, 8)
         return f.transpose(0, 2, 1).reshape(planes * 8, n3).copy()
+
+    def surrogate_train_init(self, sub: int, weights: np.ndarray, substeps: int = 50, rate_scale: float = 0.1) -> None:
+        w = np.ascontiguousarray(weights, np.float32).reshape(-1)
+        self._check(self.lib.gell_surrogate_train_init(self.h, sub, P(w.ctypes.data), w.size, substeps, rate_scale),
+                    "gell_surrogate_train_init")
+
+    def surrogate_train_pair(self, sub: int, lr: float, want_loss: bool = True) -> float | None:
+        """One training pair from the current state (see gell_surrogate_train_pair)."""
+        loss = ctypes.c_float()
+        self._check(self.lib.gell_surrogate_train_pair(self.h, sub, lr, ctypes.byref(loss) if want_loss else None),
+                    "gell_surrogate_train_pair")
+        return float(loss.value) if want_loss else None
+
+    def surrogate_train_read(self, sub: int, which: int) -> np.ndarray:
+        """which 0: master weights, 1: last gradient, 2: last target field (N^3)."""
+        if which == 2:
+            P_ = (self.N + 3) // 4 * 4
+            raw = np.zeros(P_ * self.N * self.N, np.float32)
+            self._check(self.lib.gell_surrogate_train_read(self.h, sub, 2, P(raw.ctypes.data), raw.size),
+                        "gell_surrogate_train_read")
+            return raw.reshape(self.N, self.N, P_)[:, :, :self.N].reshape(-1).copy()
+        out = np.zeros(self.lib.gell_surrogate_weight_count(), np.float32)
+        self._check(self.lib.gell_surrogate_train_read(self.h, sub, which, P(out.ctypes.data), out.size),
+                    "gell_surrogate_train_read")
+        return out
 
     # -- parity support
     def _dump(self, what: int, arg: int, dtype, count: int) -> np.ndarray:

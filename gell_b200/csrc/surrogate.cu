@@ -47,14 +47,18 @@ constexpr int kLayers = 10;                  // conv_in, 4 x (conv_a, conv_b), c
 constexpr int kHidden = 32;
 constexpr int kInCh = 3;
 
-enum ConvMode { kRelu = 0, kResidual = 1, kField = 2 };
+// Epilogues: forward (kRelu, kResidual, kField) and the data gradients of the backward pass
+// (kLinear: the gradient of a linear layer's input; kMask: times [aux > 0], the ReLU's gradient
+// with aux = the ReLU's stored output; kResMask: residual add, then times [aux > 0]).
+enum ConvMode { kRelu = 0, kResidual = 1, kField = 2, kLinear = 3, kMask = 4, kResMask = 5 };
 
 struct ConvArgs {
     CUtensorMap in;                 // 5-D map {8, N, N, N, planes}, box {8, 130, 1, 1, planes}
     const uint8_t* w;               // packed weights, the shared-memory image
     const float* bias;              // NOUT
     uint4* out;                     // planes (kRelu, kResidual)
-    const uint4* res;               // residual planes (kResidual; may equal out)
+    const uint4* res;               // residual planes (kResidual, kResMask; may equal out)
+    const uint4* aux;               // mask planes (kMask, kResMask): a channel passes where aux > 0
     float* field_out;               // pitched field (kField)
     const float* field_in;          // pitched field (kField)
     int N, P;
@@ -191,7 +195,7 @@ __device__ __forceinline__ void store_tile(const ConvArgs& a, const uint32_t (&v
         for (int n = 0; n < NOUT; ++n) f[n] = __uint_as_float(v[n]) + bias[n];
 #pragma unroll
         for (int pl = 0; pl < NOUT / 8; ++pl) {
-            if constexpr (MODE == kResidual) {
+            if constexpr (MODE == kResidual || MODE == kResMask) {
                 const uint4 r = a.res[pl * a.nvox + vox];
                 const uint32_t rr[4] = {r.x, r.y, r.z, r.w};
 #pragma unroll
@@ -200,7 +204,18 @@ __device__ __forceinline__ void store_tile(const ConvArgs& a, const uint32_t (&v
                     f[8 * pl + 2 * j] += u.x;
                     f[8 * pl + 2 * j + 1] += u.y;
                 }
-            } else {
+            }
+            if constexpr (MODE == kMask || MODE == kResMask) {
+                const uint4 m = a.aux[pl * a.nvox + vox];
+                const uint32_t mm[4] = {m.x, m.y, m.z, m.w};
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const float2 u = unpack_bf16(mm[j]);
+                    if (!(u.x > 0.f)) f[8 * pl + 2 * j] = 0.f;
+                    if (!(u.y > 0.f)) f[8 * pl + 2 * j + 1] = 0.f;
+                }
+            }
+            if constexpr (MODE == kRelu) {
 #pragma unroll
                 for (int j = 0; j < 8; ++j) f[8 * pl + j] = fmaxf(f[8 * pl + j], 0.f);
             }
@@ -501,6 +516,248 @@ __global__ void __launch_bounds__(192, 1) k_conv3_ring(const __grid_constant__ C
     }
 }
 
+// ---------------------------------------------------------------- weight gradients
+// k_wgrad (32 -> 32 layers, tcgen05): dW[co][ci][tap] = sum over voxels v of X[ci, v + tap] * G[co, v]
+// (X = the layer's input, G = the gradient of its output, zero outside the grid).  The voxels are
+// the K dimension, so both operands are read MN-major from the 8-channel planes as staged (8
+// channels of one voxel = 16 contiguous bytes, consecutive voxels 16 bytes apart: the canonical
+// no-swizzle MN-major layout, channel groups SBO apart, voxel groups of 8 LBO = 128 bytes apart).
+// Per tile (128 voxels of one x-line): the 9 runs of X (130 voxels, 4 planes) and the 128-voxel
+// run of G (4 planes); A = four consecutive runs r0..r0+3 as M = 128 rows (run, ci) (the runs of a
+// stage are 4 * 2080 bytes apart, so rows keep one stride), moved by dx voxels for tap dx; B = G.
+// 3 row groups x 3 dx x 8 blocks of 16 voxels = 72 MMAs per tile into 9 TMEM accumulators (288
+// columns) that persist over all tiles of the CTA; rows 9-11 of the last group read past the stage
+// into other staged data and are discarded.  At the end each CTA writes its partial sums.
+constexpr int kWgRunB = 4 * kRunPlaneB;            // 8320
+constexpr int kWgXB = 9 * kWgRunB;                  // 74,880
+constexpr int kWgGB = 4 * kTileM * 16;              // 8,192
+constexpr int kWgStageB = kWgXB + kWgGB;            // 83,072
+constexpr int kWgTail = 3 * kWgRunB;                // room for the discarded rows of the last stage
+constexpr int kWgBars = 2 * kWgStageB + kWgTail;
+constexpr int kWgBytes = kWgBars + 5 * 8 + 16;
+
+__host__ __device__ constexpr uint32_t idesc_bf16_mn(int n) {
+    return idesc_bf16(n) | (1u << 15) | (1u << 16);
+}
+
+struct WgradArgs {
+    CUtensorMap x;  // {8, N, N, N, 4}, box {8, 130, 1, 1, 4}
+    CUtensorMap g;  // {8, N, N, N, 4}, box {8, 128, 1, 1, 4}
+    float* partial; // [gridDim.x][32 co][32 ci][27]
+    int N, tiles_x;
+    long long tiles;
+    int* err;
+};
+
+__global__ void __launch_bounds__(192, 1) k_wgrad(const __grid_constant__ WgradArgs a) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kWgBars);
+    uint64_t* full = bars;
+    uint64_t* empty = bars + 2;
+    uint64_t* done = bars + 4;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 5);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+        }
+        mbar_init(done, 1);
+        fence_mbar_init();
+    }
+    if (warp == 1) tmem_alloc(tslot, 512);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const long long T = a.tiles;
+    ConvArgs geo{};
+    geo.N = a.N;
+    geo.tiles_x = a.tiles_x;
+    if (warp == 0) {
+        if (lane == 0) {
+            int k = 0;
+            for (long long t = blockIdx.x; t < T; t += gridDim.x, ++k) {
+                const int s = k & 1;
+                if (k >= 2 && !mbar_wait1(&empty[s], ((k >> 1) - 1) & 1, a.err, 31)) break;
+                int x0, y, z;
+                tile_of(geo, t, x0, y, z);
+                uint8_t* st = smem + s * kWgStageB;
+                mbar_arrive_expect(&full[s], (uint32_t)(kWgXB + kWgGB));
+                for (int r = 0; r < 9; ++r)
+                    tma_load_5d(st + r * kWgRunB, &a.x, 0, x0 - 1, y + r % 3 - 1, z + r / 3 - 1, 0, &full[s]);
+                tma_load_5d(st + kWgXB, &a.g, 0, x0, y, z, 0, &full[s]);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_bf16_mn(32);
+            int k = 0;
+            for (long long t = blockIdx.x; t < T; t += gridDim.x, ++k) {
+                const int s = k & 1;
+                if (!mbar_wait1(&full[s], (k >> 1) & 1, a.err, 32)) break;
+                tc_fence_after();
+                const uint32_t sb = smem_u32(smem + s * kWgStageB);
+                const uint64_t a0 = sdesc(sb, 128, kRunPlaneB);         // LBO = voxel groups, SBO = channel groups
+                const uint64_t b0 = sdesc(sb + kWgXB, 128, kTileM * 16);
+#pragma unroll
+                for (int rg = 0; rg < 3; ++rg)
+#pragma unroll
+                    for (int dx = 0; dx < 3; ++dx)
+#pragma unroll
+                        for (int kb = 0; kb < 8; ++kb) {
+                            const uint32_t ao = (4 * rg * kWgRunB + (dx + 16 * kb) * 16) >> 4;
+                            const uint32_t bo = (16 * kb * 16) >> 4;
+                            mma_bf16(tmem + (uint32_t)(32 * (3 * rg + dx)), a0 + ao, b0 + bo, idesc,
+                                     (k > 0 || kb > 0) ? 1u : 0u);
+                        }
+                mma_commit(&empty[s]);
+            }
+            mma_commit(done);
+        }
+    } else {
+        // read the 9 accumulators once every MMA of the CTA has finished
+        const int q = warp & 3;
+        if (mbar_wait(done, 0, a.err, 33, 1 << 26)) {
+            tc_fence_after();
+            float* out = a.partial + (size_t)blockIdx.x * (32 * 32 * 27);
+            const bool any = blockIdx.x < T;
+            for (int j = 0; j < 9; ++j) {
+                const int rg = j / 3, dx = j % 3;
+                uint32_t v[32];
+                tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(32 * j), v);
+                tmem_wait_ld();
+                const int r = 4 * rg + q;  // lane 32q + ci is row (run r, ci)
+                if (r < 9) {
+                    const int tap = 3 * r + dx;
+#pragma unroll
+                    for (int co = 0; co < 32; ++co)
+                        out[((size_t)co * 32 + lane) * 27 + tap] = any ? __uint_as_float(v[co]) : 0.f;
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        __syncwarp();
+        tc_fence_after();
+        tmem_dealloc(tmem, 512);
+    }
+}
+
+// Weight gradients of the thin layers on the CUDA cores (the first layer: 3 input channels; the
+// last: one output channel).  A block takes one x-line at a time: the line's gradient run and, plane
+// by plane, the 9 input runs (130 voxels) go to shared memory as fp32; thread t owns the real
+// weights w = t, t + blockDim, ... in the layer's [co][ci][tap] order and accumulates over the
+// line's voxels and over every line the block visits; each block writes its partial sums.
+constexpr int kThinMaxW = 16;
+
+__global__ void k_wgrad_thin(const uint4* X, int cin, const uint4* G, int cout, int N, long long nvox,
+                             float* partial) {
+    extern __shared__ float sm[];
+    const int RUN = N + 2;
+    float* xs = sm;                // [9][RUN][8]
+    float* gs = sm + 9 * RUN * 8;  // [N][cout]
+    const int total = cout * cin * 27;
+    float acc[kThinMaxW];
+#pragma unroll
+    for (int j = 0; j < kThinMaxW; ++j) acc[j] = 0.f;
+    const long long lines = (long long)N * N;
+    const int xplanes = (cin + 7) / 8;
+    for (long long l = blockIdx.x; l < lines; l += gridDim.x) {
+        const int y = (int)(l % N), z = (int)(l / N);
+        __syncthreads();
+        for (int i = threadIdx.x; i < N * cout; i += blockDim.x) {
+            const int x = i / cout, co = i % cout;
+            const long long vox = x + (long long)N * (y + (long long)N * z);
+            const uint4 u = G[(co / 8) * nvox + vox];
+            const uint32_t w4[4] = {u.x, u.y, u.z, u.w};
+            const float2 f = unpack_bf16(w4[(co % 8) / 2]);
+            gs[i] = (co & 1) ? f.y : f.x;
+        }
+        for (int pl = 0; pl < xplanes; ++pl) {
+            __syncthreads();
+            for (int i = threadIdx.x; i < 9 * RUN; i += blockDim.x) {
+                const int r = i / RUN, xi = i % RUN;
+                const int xx = xi - 1, yy = y + r % 3 - 1, zz = z + r / 3 - 1;
+                uint4 u = make_uint4(0u, 0u, 0u, 0u);
+                if (xx >= 0 && xx < N && yy >= 0 && yy < N && zz >= 0 && zz < N)
+                    u = X[pl * nvox + xx + (long long)N * (yy + (long long)N * zz)];
+                const uint32_t w4[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const float2 f = unpack_bf16(w4[j]);
+                    xs[i * 8 + 2 * j] = f.x;
+                    xs[i * 8 + 2 * j + 1] = f.y;
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < kThinMaxW; ++j) {
+                const int w = threadIdx.x + j * blockDim.x;
+                if (w < total) {
+                    const int co = w / (cin * 27), ci = (w / 27) % cin, tap = w % 27;
+                    if (ci / 8 == pl) {
+                        const int r = tap / 3, dx = tap % 3;
+                        const float* xr = xs + (r * RUN + dx) * 8 + (ci % 8);
+                        float sacc = 0.f;
+                        for (int x = 0; x < N; ++x) sacc = __fmaf_rn(xr[x * 8], gs[x * cout + co], sacc);
+                        acc[j] += sacc;
+                    }
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < kThinMaxW; ++j) {
+        const int w = threadIdx.x + j * blockDim.x;
+        if (w < total) partial[(size_t)blockIdx.x * total + w] = acc[j];
+    }
+}
+
+// Sum of per-block partials: out[i] = sum_b partial[b * stride + i] (fixed order: the result does
+// not depend on scheduling).
+__global__ void k_sum_partials(const float* partial, int blocks, int n, int stride, float* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float s = 0.f;
+        for (int b = 0; b < blocks; ++b) s += partial[(size_t)b * stride + i];
+        out[i] = s;
+    }
+}
+
+// Per-channel sums over the voxels of a planes tensor (bias gradients): block partials [block][C].
+__global__ void k_channel_sums(const uint4* G, int planes, long long nvox, float* partial) {
+    __shared__ float red[8][32];
+    const int C = planes * 8;
+    for (int pl = 0; pl < planes; ++pl) {
+        float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < nvox; v += (long long)gridDim.x * blockDim.x) {
+            const uint4 u = G[pl * nvox + v];
+            const uint32_t w4[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const float2 f = unpack_bf16(w4[j]);
+                s[2 * j] += f.x;
+                s[2 * j + 1] += f.y;
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            float t = s[e];
+            for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(FULL, t, o);
+            if ((threadIdx.x & 31) == 0) red[e][threadIdx.x >> 5] = t;
+        }
+        __syncthreads();
+        if (threadIdx.x < 8) {
+            float t = 0.f;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[threadIdx.x][w];
+            partial[(size_t)blockIdx.x * C + pl * 8 + threadIdx.x] = t;
+        }
+        __syncthreads();
+    }
+}
+
 // Input planes of the operator: plane 0 = (p / b, rate * rate_scale, shell, 0, ...); plane 1 stays
 // zero (the first convolution reads 16 input channels).
 __global__ void k_pack_input(const float* p, const float* rate, Geom g, float inv_b, float rate_scale, uint4* out) {
@@ -536,6 +793,97 @@ __global__ void k_absdiff_max(const float* a, const float* b, Geom g, unsigned* 
     if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
 }
 
+// ---------------------------------------------------------------- training: packing, loss, Adam
+
+// Weight images from the fp32 master weights W[cout][cin][27] of one layer (device-side packing, so
+// a training step never leaves the GPU): the forward image (input channel 16h + 8kc + e, output
+// channel n, as pack_layer) or, with `transpose`, the image of the convolution that maps the
+// gradient of the layer's output to the gradient of its input: input channels = the layer's
+// outputs, output channels = the layer's inputs, taps mirrored (tap -> 26 - tap).
+__global__ void k_pack_w(const float* W, int cin, int cout, int cin8, int nout, int transpose, __nv_bfloat16* img) {
+    const int halves = cin8 / 2;
+    const int n_img = 27 * halves * 2 * nout * 8;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_img; i += gridDim.x * blockDim.x) {
+        const int e = i % 8, n = (i / 8) % nout, kc = (i / (8 * nout)) % 2, h = (i / (16 * nout)) % halves;
+        const int tap = i / (16 * nout * halves);
+        const int k = 16 * h + 8 * kc + e;  // input channel of the packed convolution
+        float v = 0.f;
+        if (!transpose) {
+            if (n < cout && k < cin) v = W[((size_t)n * cin + k) * 27 + tap];
+        } else {
+            if (k < cout && n < cin) v = W[((size_t)k * cin + n) * 27 + (26 - tap)];
+        }
+        img[i] = __float2bfloat16_rn(v);
+    }
+}
+__global__ void k_pack_bias(const float* b, int cout, int nout, float* out) {
+    const int i = threadIdx.x;
+    if (i < nout) out[i] = i < cout ? b[i] : 0.f;
+}
+
+// Gradient of the loss L = mean over the voxels inside the shell of ((q - y) / b)^2 with respect to
+// the last convolution's output d (q = p + b d inside): 2 (q - y) / (b n), in channel 0 of plane 0
+// of the gradient planes; zero on the shell.  Block partial sums of ((q - y) / b)^2 go to `loss`.
+__global__ void k_loss_grad(const float* q, const float* y, Geom g, float b, float inv_n, uint4* gd, float* loss) {
+    __shared__ float red[32];
+    const int N = g.N;
+    const long long nvox = (long long)N * N * N;
+    float acc = 0.f;
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < nvox; v += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(v % N);
+        const long long yz = v / N;
+        const int yy = (int)(yz % N), zz = (int)(yz / N);
+        const bool shell = x < 2 || x > N - 3 || yy < 2 || yy > N - 3 || zz < 2 || zz > N - 3;
+        float gr = 0.f;
+        if (!shell) {
+            const long long pi = x + (long long)g.P * yy + g.PN * zz;
+            const float e = (q[pi] - y[pi]) / b;
+            acc = __fmaf_rn(e, e, acc);
+            gr = 2.f * e * inv_n;
+        }
+        gd[v] = make_uint4(pack_bf16(gr, 0.f), 0u, 0u, 0u);
+    }
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(FULL, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        loss[blockIdx.x] = t;
+    }
+}
+
+// Sum of squares of the gradient (for clipping by its global norm): one block.
+__global__ void k_sumsq(const float* g, long long n, float* out) {
+    __shared__ float red[32];
+    float acc = 0.f;
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) acc = __fmaf_rn(g[i], g[i], acc);
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(FULL, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        *out = t;
+    }
+}
+
+// Adam (Kingma & Ba, ICLR 2015) with bias correction, on the gradient scaled to global norm
+// <= clip: m = b1 m + (1 - b1) g; v = b2 v + (1 - b2) g^2; w -= lr (m / bc1) / (sqrt(v / bc2) + eps).
+__global__ void k_adam(float* w, const float* g, float* m, float* v, long long n, const float* sumsq, float clip,
+                       float lr, float b1, float b2, float eps, float bc1, float bc2) {
+    const float norm = sqrtf(*sumsq);
+    const float sc = norm > clip ? clip / norm : 1.f;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float gi = g[i] * sc;
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        w[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+    }
+}
+
 // Layer table: input planes, output channels (padded), mode.
 struct LayerShape {
     int cin, cout, cin8, nout;
@@ -548,6 +896,27 @@ constexpr LayerShape kShape[kLayers] = {
 }  // namespace
 
 // ---------------------------------------------------------------- host state
+
+// Training state of one substrate's operator (gell_surrogate_train_*): fp32 master weights in the
+// layout of gell_surrogate_load, their gradient and Adam moments, the images of the data-gradient
+// convolutions, every activation of the forward pass and the gradient planes.
+struct TrainState {
+    long long count = 0;
+    long long off_w[kLayers] = {}, off_b[kLayers] = {};
+    float *master = nullptr, *grad = nullptr, *m = nullptr, *v = nullptr;
+    float* partial = nullptr;    // block partial sums
+    long long partial_n = 0;
+    float* zero_bias = nullptr;  // 32 zeros
+    float* scal = nullptr;       // [0] gradient sum of squares, [1] loss, [2..] loss partials
+    float* hloss = nullptr;      // pinned
+    uint8_t* wt[kLayers] = {};   // data-gradient images (layers 1..9)
+    uint4* hb[5] = {};
+    uint4* tb[4] = {};
+    uint4 *gh = nullptr, *gu = nullptr, *gd = nullptr;
+    float* tgt = nullptr;        // the plain solver's field after the substeps (pitched)
+    CUtensorMap mh[5], mt[4], mgd, mgh, mgu, mgh_g, mgu_g;
+    int step = 0;
+};
 
 struct SurrogateState {
     int substeps = 0;
@@ -562,8 +931,8 @@ struct SurrogateState {
     unsigned* dmax = nullptr;   // judge scratch
     unsigned* hmax = nullptr;   // pinned host copy
     CUtensorMap map_in, map_h, map_t;
-    long long conv_launches = 0;
     double conv_flops = 0;      // algorithmic FLOPs of one inference (real channels only)
+    struct TrainState* train = nullptr;
 };
 
 void surrogate_free(gell_ctx* c) {
@@ -576,12 +945,22 @@ void surrogate_free(gell_ctx* c) {
         for (void* p : {(void*)s->in, (void*)s->h, (void*)s->t, (void*)s->ph, (void*)s->backup, (void*)s->dmax})
             if (p) cudaFree(p);
         if (s->hmax) cudaFreeHost(s->hmax);
+        if (TrainState* t = s->train) {
+            for (void* p : {(void*)t->master, (void*)t->grad, (void*)t->m, (void*)t->v, (void*)t->partial,
+                            (void*)t->zero_bias, (void*)t->scal, (void*)t->gh, (void*)t->gu, (void*)t->gd, (void*)t->tgt})
+                if (p) cudaFree(p);
+            for (auto* p : t->wt) if (p) cudaFree(p);
+            for (auto* p : t->hb) if (p) cudaFree(p);
+            for (auto* p : t->tb) if (p) cudaFree(p);
+            if (t->hloss) cudaFreeHost(t->hloss);
+            delete t;
+        }
         delete s;
         s = nullptr;
     }
 }
 
-static gell_status plane_map(gell_ctx* c, CUtensorMap* m, void* base, int planes) {
+static gell_status plane_map(gell_ctx* c, CUtensorMap* m, void* base, int planes, int box_x = kRunVox) {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     if (!encode) {
         cudaDriverEntryPointQueryResult q;
@@ -594,7 +973,7 @@ static gell_status plane_map(gell_ctx* c, CUtensorMap* m, void* base, int planes
     const cuuint64_t N = (cuuint64_t)c->g.N;
     const cuuint64_t dims[5] = {8, N, N, N, (cuuint64_t)planes};
     const cuuint64_t strides[4] = {16, 16 * N, 16 * N * N, 16 * N * N * N};
-    const cuuint32_t box[5] = {8, (cuuint32_t)kRunVox, 1, 1, (cuuint32_t)planes};
+    const cuuint32_t box[5] = {8, (cuuint32_t)box_x, 1, 1, (cuuint32_t)planes};
     const cuuint32_t es[5] = {1, 1, 1, 1, 1};
     CUresult r = encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, base, dims, strides, box, es,
                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -629,8 +1008,9 @@ static void pack_layer(const float* W, const LayerShape& s, std::vector<uint16_t
 }
 
 template <int CIN8, int NOUT, int MODE>
-static gell_status launch_conv(gell_ctx* c, const char* name, SurrogateState* S, const CUtensorMap& in, int layer, uint4* out,
-                               const uint4* res, float* fout, const float* fin, float scale, float bval) {
+static gell_status launch_conv(gell_ctx* c, const char* name, const CUtensorMap& in, const uint8_t* w, const float* bias,
+                               uint4* out, const uint4* res, const uint4* aux, float* fout, const float* fin, float scale,
+                               float bval) {
     using L = ConvSmem<CIN8, NOUT>;
     using R = RingSmem<CIN8, NOUT>;
     // the shared-memory opt-in is a per-device attribute; setting it is cheap, so every launch does
@@ -642,10 +1022,11 @@ static gell_status launch_conv(gell_ctx* c, const char* name, SurrogateState* S,
                                           L::kBytes));
     ConvArgs a{};
     a.in = in;
-    a.w = S->w[layer];
-    a.bias = S->bias[layer];
+    a.w = w;
+    a.bias = bias;
     a.out = out;
     a.res = res;
+    a.aux = aux;
     a.field_out = fout;
     a.field_in = fin;
     a.N = c->g.N;
@@ -667,7 +1048,6 @@ static gell_status launch_conv(gell_ctx* c, const char* name, SurrogateState* S,
         const int grid = (int)(a.tiles < sms ? a.tiles : sms);
         GELL_KERNEL(c, name, (k_conv3<CIN8, NOUT, MODE><<<grid, 192, L::kBytes, c->stream>>>(a)));
     }
-    S->conv_launches++;
     return GELL_OK;
 }
 
@@ -685,14 +1065,158 @@ static gell_status run_layers(gell_ctx* c, int sub, SurrogateState* S, int layer
                                                                                  S->rate_scale, S->in)));
     gell_status st = GELL_OK;
     for (int l = 0; l < layers && st == GELL_OK; ++l) {
-        if (l == 0) st = launch_conv<2, 32, kRelu>(c, "k_conv3_in", S, S->map_in, 0, S->h, nullptr, nullptr, nullptr, 0.f, 0.f);
-        else if (l == kLayers - 1) st = launch_conv<4, 16, kField>(c, "k_conv3_out", S, S->map_h, l, nullptr, nullptr, S->ph, Su.p, b, b);
-        else if (l & 1) st = launch_conv<4, 32, kRelu>(c, "k_conv3_hidden", S, S->map_h, l, S->t, nullptr, nullptr, nullptr, 0.f, 0.f);
-        else st = launch_conv<4, 32, kResidual>(c, "k_conv3_hidden", S, S->map_t, l, S->h, S->h, nullptr, nullptr, 0.f, 0.f);
+        const uint8_t* w = S->w[l];
+        const float* bi = S->bias[l];
+        if (l == 0)
+            st = launch_conv<2, 32, kRelu>(c, "k_conv3_in", S->map_in, w, bi, S->h, nullptr, nullptr, nullptr, nullptr, 0.f, 0.f);
+        else if (l == kLayers - 1)
+            st = launch_conv<4, 16, kField>(c, "k_conv3_out", S->map_h, w, bi, nullptr, nullptr, nullptr, S->ph, Su.p, b, b);
+        else if (l & 1)
+            st = launch_conv<4, 32, kRelu>(c, "k_conv3_hidden", S->map_h, w, bi, S->t, nullptr, nullptr, nullptr, nullptr, 0.f, 0.f);
+        else
+            st = launch_conv<4, 32, kResidual>(c, "k_conv3_hidden", S->map_t, w, bi, S->h, S->h, nullptr, nullptr, nullptr, 0.f, 0.f);
     }
     return st;
 }
 static gell_status infer(gell_ctx* c, int sub, SurrogateState* S) { return run_layers(c, sub, S, kLayers); }
+
+// Shapes of the data-gradient convolution of layer l: input planes (the layer's outputs, padded to
+// 16 channels) and outputs (the layer's inputs).
+static int dgrad_cin8(int l) { return kShape[l].cout <= 16 ? 2 : 4; }
+static int dgrad_nout(int l) { return kShape[l].cin <= 16 ? 16 : 32; }
+
+static gell_status repack(gell_ctx* c, SurrogateState* S) {
+    TrainState* T = S->train;
+    for (int l = 0; l < kLayers; ++l) {
+        const LayerShape& sh = kShape[l];
+        GELL_KERNEL(c, "k_pack_w", (k_pack_w<<<64, 256, 0, c->stream>>>(T->master + T->off_w[l], sh.cin, sh.cout, sh.cin8,
+                                                                         sh.nout, 0, (__nv_bfloat16*)S->w[l])));
+        GELL_KERNEL(c, "k_pack_bias", (k_pack_bias<<<1, 32, 0, c->stream>>>(T->master + T->off_b[l], sh.cout, sh.nout, S->bias[l])));
+        if (l >= 1)
+            GELL_KERNEL(c, "k_pack_w", (k_pack_w<<<64, 256, 0, c->stream>>>(T->master + T->off_w[l], sh.cin, sh.cout,
+                                                                             dgrad_cin8(l), dgrad_nout(l), 1,
+                                                                             (__nv_bfloat16*)T->wt[l])));
+    }
+    return GELL_OK;
+}
+
+static int thin_blocks() { return 148 * 4; }
+
+// Weight gradient of layer l into T->grad (the layer's block): tcgen05 for the 32 -> 32 layers,
+// CUDA cores for the thin first and last layers; bias gradient = per-channel sums of G.
+static gell_status wgrad_layer(gell_ctx* c, SurrogateState* S, int l, const CUtensorMap* xmap, const uint4* X,
+                               const CUtensorMap* gmap, const uint4* G, int gplanes) {
+    TrainState* T = S->train;
+    const LayerShape& sh = kShape[l];
+    const int N = c->g.N;
+    const int nw = sh.cout * sh.cin * 27;
+    if (sh.cin == kHidden && sh.cout == kHidden) {
+        WgradArgs a{};
+        a.x = *xmap;
+        a.g = *gmap;
+        a.partial = T->partial;
+        a.N = N;
+        a.tiles_x = (N + kTileM - 1) / kTileM;
+        a.tiles = (long long)a.tiles_x * N * N;
+        a.err = c->dev_err;
+        int sms = 0;
+        GELL_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+        const int grid = (int)(a.tiles < sms ? a.tiles : sms);
+        GELL_CUDA(c, cudaFuncSetAttribute(k_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgBytes));
+        GELL_KERNEL(c, "k_wgrad", (k_wgrad<<<grid, 192, kWgBytes, c->stream>>>(a)));
+        GELL_KERNEL(c, "k_sum_partials", (k_sum_partials<<<(nw + 255) / 256, 256, 0, c->stream>>>(T->partial, grid, nw, nw,
+                                                                                                  T->grad + T->off_w[l])));
+    } else {
+        const int smem = (9 * (N + 2) * 8 + N * sh.cout) * 4;
+        GELL_CUDA(c, cudaFuncSetAttribute(k_wgrad_thin, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        GELL_KERNEL(c, "k_wgrad_thin", (k_wgrad_thin<<<thin_blocks(), 256, smem, c->stream>>>(X, sh.cin, G, sh.cout, N,
+                                                                                                c->nvox, T->partial)));
+        GELL_KERNEL(c, "k_sum_partials", (k_sum_partials<<<(nw + 255) / 256, 256, 0, c->stream>>>(
+                                              T->partial, thin_blocks(), nw, nw, T->grad + T->off_w[l])));
+    }
+    const int C = gplanes * 8;
+    GELL_KERNEL(c, "k_channel_sums", (k_channel_sums<<<thin_blocks(), 256, 0, c->stream>>>(G, gplanes, c->nvox, T->partial)));
+    GELL_KERNEL(c, "k_sum_partials", (k_sum_partials<<<1, 32, 0, c->stream>>>(T->partial, thin_blocks(), sh.cout, C,
+                                                                              T->grad + T->off_b[l])));
+    return GELL_OK;
+}
+
+// One training pair: the plain solver advances the field by the operator's substeps (the target),
+// the operator runs from the field before them with every activation kept, the loss gradient goes
+// back through the ten layers (data gradients on tcgen05, weight gradients as above), Adam updates
+// the master weights, the images are repacked, and the field is left at the target.
+static gell_status train_pair(gell_ctx* c, int sub, SurrogateState* S, float lr, float* loss_out) {
+    TrainState* T = S->train;
+    Substrate& Su = c->subs[sub];
+    const float b = Su.s.boundary;
+    const size_t fb = (size_t)c->nvox_p * 4;
+    GELL_CUDA(c, cudaMemcpyAsync(S->backup, Su.p, fb, cudaMemcpyDeviceToDevice, c->stream));
+    gell_status st = lod_solver(c, sub, S->substeps);
+    if (st != GELL_OK) return st;
+    GELL_CUDA(c, cudaMemcpyAsync(T->tgt, Su.p, fb, cudaMemcpyDeviceToDevice, c->stream));
+    GELL_CUDA(c, cudaMemcpyAsync(Su.p, S->backup, fb, cudaMemcpyDeviceToDevice, c->stream));
+
+    // forward, every activation kept
+    const int pb = blocks_for(c->nvox, 256);
+    GELL_KERNEL(c, "k_pack_input", (k_pack_input<<<pb < 148 * 16 ? pb : 148 * 16, 256, 0, c->stream>>>(
+                                        Su.p, Su.rate, c->g, 1.f / b, S->rate_scale, S->in)));
+    st = launch_conv<2, 32, kRelu>(c, "k_conv3_in", S->map_in, S->w[0], S->bias[0], T->hb[0], nullptr, nullptr, nullptr,
+                                   nullptr, 0.f, 0.f);
+    for (int k = 0; k < 4 && st == GELL_OK; ++k) {
+        st = launch_conv<4, 32, kRelu>(c, "k_conv3_hidden", T->mh[k], S->w[2 * k + 1], S->bias[2 * k + 1], T->tb[k],
+                                       nullptr, nullptr, nullptr, nullptr, 0.f, 0.f);
+        if (st == GELL_OK)
+            st = launch_conv<4, 32, kResidual>(c, "k_conv3_hidden", T->mt[k], S->w[2 * k + 2], S->bias[2 * k + 2],
+                                               T->hb[k + 1], T->hb[k], nullptr, nullptr, nullptr, 0.f, 0.f);
+    }
+    if (st == GELL_OK)
+        st = launch_conv<4, 16, kField>(c, "k_conv3_out", T->mh[4], S->w[9], S->bias[9], nullptr, nullptr, nullptr, S->ph,
+                                        Su.p, b, b);
+    if (st != GELL_OK) return st;
+
+    // loss and its gradient
+    const long long inner = (long long)(c->g.N - 4) * (c->g.N - 4) * (c->g.N - 4);
+    const int lb = 148 * 8;
+    GELL_KERNEL(c, "k_loss_grad", (k_loss_grad<<<lb, 256, 0, c->stream>>>(S->ph, T->tgt, c->g, b, 1.f / (float)inner, T->gd,
+                                                                          T->scal + 2)));
+    GELL_KERNEL(c, "k_sum_partials", (k_sum_partials<<<1, 32, 0, c->stream>>>(T->scal + 2, lb, 1, 1, T->scal + 1)));
+
+    // backward
+    if ((st = wgrad_layer(c, S, 9, nullptr, T->hb[4], nullptr, T->gd, 1)) != GELL_OK) return st;
+    st = launch_conv<2, 32, kLinear>(c, "k_conv3_dgrad", T->mgd, T->wt[9], T->zero_bias, T->gh, nullptr, nullptr, nullptr,
+                                     nullptr, 0.f, 0.f);
+    for (int k = 3; k >= 0 && st == GELL_OK; --k) {
+        if ((st = wgrad_layer(c, S, 2 * k + 2, &T->mt[k], T->tb[k], &T->mgh_g, T->gh, 4)) != GELL_OK) return st;
+        st = launch_conv<4, 32, kMask>(c, "k_conv3_dgrad", T->mgh, T->wt[2 * k + 2], T->zero_bias, T->gu, nullptr,
+                                       T->tb[k], nullptr, nullptr, 0.f, 0.f);
+        if (st != GELL_OK) return st;
+        if ((st = wgrad_layer(c, S, 2 * k + 1, &T->mh[k], T->hb[k], &T->mgu_g, T->gu, 4)) != GELL_OK) return st;
+        if (k > 0)
+            st = launch_conv<4, 32, kResidual>(c, "k_conv3_dgrad", T->mgu, T->wt[2 * k + 1], T->zero_bias, T->gh, T->gh,
+                                               nullptr, nullptr, nullptr, 0.f, 0.f);
+        else
+            st = launch_conv<4, 32, kResMask>(c, "k_conv3_dgrad", T->mgu, T->wt[1], T->zero_bias, T->gh, T->gh, T->hb[0],
+                                              nullptr, nullptr, 0.f, 0.f);
+    }
+    if (st != GELL_OK) return st;
+    if ((st = wgrad_layer(c, S, 0, nullptr, S->in, nullptr, T->gh, 4)) != GELL_OK) return st;
+
+    // Adam on the clipped gradient, new images
+    GELL_KERNEL(c, "k_sumsq", (k_sumsq<<<1, 1024, 0, c->stream>>>(T->grad, T->count, T->scal)));
+    T->step++;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float bc1 = 1.f - powf(b1, (float)T->step), bc2 = 1.f - powf(b2, (float)T->step);
+    GELL_KERNEL(c, "k_adam", (k_adam<<<64, 256, 0, c->stream>>>(T->master, T->grad, T->m, T->v, T->count, T->scal, 1.f, lr,
+                                                                b1, b2, 1e-8f, bc1, bc2)));
+    if ((st = repack(c, S)) != GELL_OK) return st;
+    GELL_CUDA(c, cudaMemcpyAsync(Su.p, T->tgt, fb, cudaMemcpyDeviceToDevice, c->stream));
+    if (loss_out) {
+        GELL_CUDA(c, cudaMemcpyAsync(T->hloss, T->scal + 1, 4, cudaMemcpyDeviceToHost, c->stream));
+        GELL_CUDA(c, cudaStreamSynchronize(c->stream));
+        *loss_out = *T->hloss / (float)inner;
+    }
+    return GELL_OK;
+}
 
 }  // namespace gell
 
@@ -799,6 +1323,78 @@ gell_status gell_lod_surrogate(gell_ctx* c, int sub, int* accepted, float* resid
     }
     GELL_CUDA(c, cudaMemcpyAsync(Su.p, S->backup, fb, cudaMemcpyDeviceToDevice, c->stream));
     return lod_solver(c, sub, S->substeps);
+}
+
+gell_status gell_surrogate_train_init(gell_ctx* c, int sub, const float* weights, long long count, int substeps,
+                                      float rate_scale) {
+    GELL_RANGE("gell_surrogate_train_init");
+    gell_status st = gell_surrogate_load(c, sub, weights, count, substeps, rate_scale, 0.f);
+    if (st != GELL_OK) return st;
+    SurrogateState* S = c->sur[sub];
+    if (!S->train) {
+        TrainState* T = new TrainState();
+        S->train = T;
+        T->count = count;
+        long long off = 0;
+        for (int l = 0; l < kLayers; ++l) {
+            T->off_w[l] = off;
+            off += (long long)kShape[l].cout * kShape[l].cin * 27;
+            T->off_b[l] = off;
+            off += kShape[l].cout;
+        }
+        const size_t plane = (size_t)c->nvox * 16, field = (size_t)c->nvox_p * 4;
+        T->partial_n = 148LL * 32 * 32 * 27;
+        bool ok = cudaMalloc(&T->master, count * 4) == cudaSuccess && cudaMalloc(&T->grad, count * 4) == cudaSuccess &&
+                  cudaMalloc(&T->m, count * 4) == cudaSuccess && cudaMalloc(&T->v, count * 4) == cudaSuccess &&
+                  cudaMalloc(&T->partial, T->partial_n * 4) == cudaSuccess &&
+                  cudaMalloc(&T->zero_bias, 32 * 4) == cudaSuccess &&
+                  cudaMalloc(&T->scal, (2 + 148 * 8) * 4) == cudaSuccess && cudaMallocHost(&T->hloss, 4) == cudaSuccess &&
+                  cudaMalloc(&T->gh, 4 * plane) == cudaSuccess && cudaMalloc(&T->gu, 4 * plane) == cudaSuccess &&
+                  cudaMalloc(&T->gd, 2 * plane) == cudaSuccess && cudaMalloc(&T->tgt, field) == cudaSuccess;
+        for (int k = 0; ok && k < 5; ++k) ok = cudaMalloc(&T->hb[k], 4 * plane) == cudaSuccess;
+        for (int k = 0; ok && k < 4; ++k) ok = cudaMalloc(&T->tb[k], 4 * plane) == cudaSuccess;
+        for (int l = 1; ok && l < kLayers; ++l)
+            ok = cudaMalloc(&T->wt[l], (size_t)27 * (dgrad_cin8(l) / 2) * 2 * dgrad_nout(l) * 8 * 2) == cudaSuccess;
+        if (!ok) return fail(c, GELL_ERR_ALLOC, "surrogate training buffers (46 planes of 16 bytes per voxel)");
+        GELL_CUDA(c, cudaMemset(T->zero_bias, 0, 32 * 4));
+        GELL_CUDA(c, cudaMemset(T->gd, 0, 2 * plane));
+        for (int k = 0; k < 5 && st == GELL_OK; ++k) st = plane_map(c, &T->mh[k], T->hb[k], 4);
+        for (int k = 0; k < 4 && st == GELL_OK; ++k) st = plane_map(c, &T->mt[k], T->tb[k], 4);
+        if (st == GELL_OK) st = plane_map(c, &T->mgd, T->gd, 2);
+        if (st == GELL_OK) st = plane_map(c, &T->mgh, T->gh, 4);
+        if (st == GELL_OK) st = plane_map(c, &T->mgu, T->gu, 4);
+        if (st == GELL_OK) st = plane_map(c, &T->mgh_g, T->gh, 4, kTileM);
+        if (st == GELL_OK) st = plane_map(c, &T->mgu_g, T->gu, 4, kTileM);
+        if (st != GELL_OK) return st;
+    }
+    TrainState* T = S->train;
+    T->step = 0;
+    GELL_CUDA(c, cudaMemcpy(T->master, weights, count * 4, cudaMemcpyHostToDevice));
+    GELL_CUDA(c, cudaMemset(T->m, 0, count * 4));
+    GELL_CUDA(c, cudaMemset(T->v, 0, count * 4));
+    return repack(c, S);
+}
+
+gell_status gell_surrogate_train_pair(gell_ctx* c, int sub, float lr, float* loss) {
+    GELL_RANGE("gell_surrogate_train_pair");
+    if (!c || sub < 0 || sub >= (int)c->subs.size() || !c->sur[sub] || !c->sur[sub]->train) return GELL_ERR_INVALID_ARG;
+    return train_pair(c, sub, c->sur[sub], lr, loss);
+}
+
+gell_status gell_surrogate_train_read(gell_ctx* c, int sub, int which, float* host, long long count) {
+    if (!c || !host || sub < 0 || sub >= (int)c->subs.size() || !c->sur[sub] || !c->sur[sub]->train)
+        return GELL_ERR_INVALID_ARG;
+    TrainState* T = c->sur[sub]->train;
+    if (which == 2) {
+        if (count != c->nvox_p) return GELL_ERR_INVALID_ARG;
+        GELL_CUDA(c, cudaMemcpyAsync(host, T->tgt, (size_t)count * 4, cudaMemcpyDeviceToHost, c->stream));
+    } else {
+        if (count != T->count || (which != 0 && which != 1)) return GELL_ERR_INVALID_ARG;
+        GELL_CUDA(c, cudaMemcpyAsync(host, which == 0 ? T->master : T->grad, (size_t)count * 4, cudaMemcpyDeviceToHost,
+                                     c->stream));
+    }
+    GELL_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GELL_OK;
 }
 
 gell_status gell_surrogate_run_layers(gell_ctx* c, int sub, int layers) {

@@ -1,8 +1,8 @@
 """The learned LOD surrogate: weight files, the operator as a PyTorch module (for fitting), training
 pairs from the plain solver, and the judge's calibration.
 
-The operator itself runs in the library (gell_surrogate_load / gell_lod_surrogate, hand-written
-tcgen05 convolutions); this module only produces its weights.  Training pairs come from the plain
+The operator, its training step and its judge run in the library (gell_surrogate_train_pair,
+gell_lod_surrogate: hand-written tcgen05 kernels); this module drives the fit and the calibration.  Training pairs come from the plain
 LOD solver (the reference's LODsolver, include/LODkernel.cuh:280-300, bit-exact in this library):
 input (p, uptake map, shell) -> p after `substeps` substeps, over seeded jittered-lattice
 spheroids with the large plain-method workload's statistics (volume fraction 0.6, radii N(5, 0.5)
@@ -66,34 +66,37 @@ def shell_mask(N: int) -> np.ndarray:
     return (s[:, None, None] | s[None, :, None] | s[None, None, :]).ravel()
 
 
-def make_torch_operator():
-    """The operator as a torch.nn.Module with the library's layer order and semantics."""
-    import torch
-    from torch import nn
+def init_weights(seed: int = 11) -> np.ndarray:
+    """Initial weights: U(-1/sqrt(fan_in), 1/sqrt(fan_in)) for every layer but the last, which is
+    zero, so the fit starts from the identity map q = p."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    parts = []
+    for l, (ci, co) in enumerate(SHAPES):
+        if l == len(SHAPES) - 1:
+            parts += [np.zeros(co * ci * 27, np.float32), np.zeros(co, np.float32)]
+        else:
+            bound = 1.0 / np.sqrt(ci * 27)
+            parts += [rng.uniform(-bound, bound, co * ci * 27).astype(np.float32),
+                      rng.uniform(-bound, bound, co).astype(np.float32)]
+    return np.concatenate(parts)
 
-    class Operator(nn.Module):
-        def __init__(self):
-            super().__init__()
-            self.convs = nn.ModuleList(nn.Conv3d(ci, co, 3, padding=1) for ci, co in SHAPES)
-            nn.init.zeros_(self.convs[-1].weight)  # starts as the identity map p -> p
-            nn.init.zeros_(self.convs[-1].bias)
 
-        def forward(self, x, p, b, shell):
-            h = torch.relu(self.convs[0](x))
-            for k in range(4):
-                t = torch.relu(self.convs[1 + 2 * k](h))
-                h = h + self.convs[2 + 2 * k](t)
-            d = self.convs[9](h)[:, 0]
-            return torch.where(shell, torch.full_like(p, b), p + b * d)
-
-        def flat_weights(self) -> np.ndarray:
-            parts = []
-            for c in self.convs:
-                parts.append(c.weight.detach().float().cpu().numpy().ravel())
-                parts.append(c.bias.detach().float().cpu().numpy().ravel())
-            return np.concatenate(parts).astype(np.float32)
-
-    return Operator()
+def seed_spheroid(sim, rng, N: int, cells: tuple[int, int], length: float, warm: tuple[int, int]) -> None:
+    """A new seeded spheroid in `sim` (cell count log-uniform in `cells`, random centre), its field
+    relaxed from the boundary value by a number of plain substeps drawn from `warm`."""
+    import gell_b200 as gb
+    L = N * length
+    n = int(np.exp(rng.uniform(np.log(cells[0]), np.log(cells[1]))))
+    a = (4.0 / 3.0 * np.pi * 125.0 / 0.6) ** (1.0 / 3.0)
+    r = a * (3.0 * n / (4.0 * np.pi)) ** (1.0 / 3.0)
+    lo, hi = r + 4 * length, L - r - 4 * length
+    centre = rng.uniform(lo, hi, 3) if hi > lo else np.full(3, L / 2)
+    c = gb.lattice_spheroid(n, centre, int(rng.integers(1 << 30)), length, N)
+    c = gb.seed_ki67_states(c, int(rng.integers(1 << 30)))
+    sim.import_cells(c)
+    sim.set_field(0, np.full(N ** 3, sim_boundary(gb), np.float32))
+    sim.PreLOD()
+    sim.LODsolver(int(rng.integers(warm[0], warm[1] + 1)), 0)
 
 
 class PairSource:
@@ -119,18 +122,7 @@ class PairSource:
         self.k = 0
 
     def _reseed(self, sim) -> None:
-        gb, N, L = self.gb, self.N, self.N * self.length
-        n = int(np.exp(self.rng.uniform(np.log(self.cells[0]), np.log(self.cells[1]))))
-        a = (4.0 / 3.0 * np.pi * 125.0 / 0.6) ** (1.0 / 3.0)
-        r = a * (3.0 * n / (4.0 * np.pi)) ** (1.0 / 3.0)
-        lo, hi = r + 4 * self.length, L - r - 4 * self.length
-        centre = self.rng.uniform(lo, hi, 3) if hi > lo else np.full(3, L / 2)
-        c = gb.lattice_spheroid(n, centre, int(self.rng.integers(1 << 30)), self.length, N)
-        c = gb.seed_ki67_states(c, int(self.rng.integers(1 << 30)))
-        sim.import_cells(c)
-        sim.set_field(0, np.full(N ** 3, sim_boundary(gb), np.float32))
-        sim.PreLOD()
-        sim.LODsolver(int(self.rng.integers(self.warm[0], self.warm[1] + 1)), 0)
+        seed_spheroid(sim, self.rng, self.N, self.cells, self.length, self.warm)
 
     def next(self):
         """(p, rate, target) as float32 arrays of N^3 values."""
@@ -160,50 +152,45 @@ def sim_boundary(gb) -> float:
 
 def train(N: int = 256, pairs: int = 2000, substeps: int = 50, rate_scale: float = 0.1, seed: int = 11,
           cells: tuple[int, int] = (150_000, 450_000), lr: float = 3e-4, max_seconds: float = float("inf"),
+          blocks: int = 4, warm: tuple[int, int] = (300, 1000), moves: tuple[int, int] = (1, 5),
           log=print) -> SurrogateWeights:
-    """Fit the operator on `pairs` pairs (one per iteration, never reused) with Adam (gradient norm
-    clipped at 1, cosine decay) on the mean squared error inside the shell, in units of the boundary
-    value; stops early after `max_seconds`.  The log compares with the identity map q = p."""
+    """Fit the operator with the library's training kernels (gell_surrogate_train_pair): one pair per
+    step, never reused, from one context that follows a seeded spheroid for `blocks` blocks (each
+    block: 1-5 mechanics steps, PreLOD, the pair) before the next spheroid replaces it.  Adam with
+    the gradient clipped to norm 1 and the rate on a cosine from `lr` to 0; the loss is the mean
+    squared error inside the shell in units of the boundary value.  Stops after `max_seconds`."""
+    import math
     import time
-    import torch
+
     import gell_b200 as gb
 
-    dev = torch.device("cuda")
-    b = sim_boundary(gb)
+    rng = np.random.Generator(np.random.Philox(seed))
     t0 = time.time()
-    cl = torch.channels_last_3d
-    net = make_torch_operator().to(dev).to(memory_format=cl)
-    opt = torch.optim.Adam(net.parameters(), lr=lr)
-    sched = torch.optim.lr_scheduler.CosineAnnealingLR(opt, pairs)
-    shell = torch.from_numpy(shell_mask(N)).to(dev).reshape(1, N, N, N)
-    inner = ~shell
-    src = PairSource(N, cells, seed, substeps)
-    try:
+    done = 0
+    with gb.Simulation(voxel_num=N, voxel_length=10.0, max_cell_num=cells[1]) as sim:
+        sim.add_substrate(gb.oxygen())
+        sim.surrogate_train_init(0, init_weights(seed), substeps, rate_scale)
+        left = 0
         for it in range(pairs):
-            p, rate, tgt = src.next()
-            pt = torch.from_numpy(p).to(dev).reshape(1, N, N, N)
-            x = torch.stack([pt / b, torch.from_numpy(rate).to(dev).reshape(1, N, N, N) * rate_scale,
-                             shell.float()], 1).contiguous(memory_format=cl)
-            y = torch.from_numpy(tgt).to(dev).reshape(1, N, N, N)
-            with torch.autocast("cuda", dtype=torch.bfloat16):
-                q = net(x, pt, b, shell)
-            err = ((q.float() - y) / b)[inner]
-            loss = (err * err).mean()
-            opt.zero_grad(set_to_none=True)
-            loss.backward()
-            torch.nn.utils.clip_grad_norm_(net.parameters(), 1.0)
-            opt.step()
-            sched.step()
-            if it % 50 == 0 or it == pairs - 1:
-                ident = ((pt - y) / b)[inner].abs().max().item()
-                log(f"pair {it} ({time.time() - t0:.0f} s): rmse {loss.sqrt().item():.3e} "
-                    f"linf {err.abs().max().item():.3e} (identity linf {ident:.3e})")
+            if left == 0:
+                seed_spheroid(sim, rng, N, cells, 10.0, warm)
+                left = blocks
+            for _ in range(int(rng.integers(moves[0], moves[1] + 1))):
+                sim.FM_update()
+            sim.PreLOD()
+            rate = 0.5 * lr * (1.0 + math.cos(math.pi * it / pairs))
+            report = it % 50 == 0 or it == pairs - 1
+            loss = sim.surrogate_train_pair(0, rate, want_loss=report)
+            left -= 1
+            done = it + 1
+            if report:
+                log(f"pair {it} ({time.time() - t0:.0f} s): rmse {math.sqrt(loss):.3e}")
             if time.time() - t0 > max_seconds:
-                log(f"stopped after {it + 1} pairs ({max_seconds:.0f} s)")
+                log(f"stopped after {done} pairs ({max_seconds:.0f} s)")
                 break
-    finally:
-        src.close()
-    return SurrogateWeights(net.flat_weights(), substeps, rate_scale, 0.0)
+        w = sim.surrogate_train_read(0, 0)
+    log(f"fit: {done} pairs in {time.time() - t0:.1f} s")
+    return SurrogateWeights(w, substeps, rate_scale, 0.0)
 
 
 def calibrate(sw: SurrogateWeights, N: int = 256, pairs: int = 64, seed: int = 1234,
@@ -298,11 +285,9 @@ def main(argv=None) -> int:
     ap.add_argument("--tol", type=float, default=0.01)
     ap.add_argument("--max-seconds", type=float, default=float("inf"))
     a = ap.parse_args(argv)
-    t0 = time.time()
     sw = train(a.N, a.pairs, a.substeps, lr=a.lr, max_seconds=a.max_seconds,
                log=lambda m: print(m, flush=True))
     t1 = time.time()
-    print(f"fit: {a.pairs} pairs in {t1 - t0:.1f} s", flush=True)
     sw.threshold, pts = calibrate(sw, a.N, a.val_pairs, tol=a.tol, log=lambda m: print(m, flush=True))
     print(f"calibration: {a.val_pairs} pairs in {time.time() - t1:.1f} s", flush=True)
     save_weights(a.out, sw)

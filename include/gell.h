@@ -363,6 +363,23 @@ gell_status gell_ensemble_sync(gell_ensemble* ens);
  * 1 = h, 2 = t, 4 x 16 bytes per voxel; 3 = the output field, pitched) — for tests.  Activations are
  * stored as planes of 8 channels: plane q holds channels 8q..8q+7 of voxel x + N*(y + N*z) as 8
  * bf16 values at byte 16*(voxel + q*N^3). */
+/* Training with the library's own kernels (no reference counterpart).
+ * gell_surrogate_train_init: loads `weights` as gell_surrogate_load does and keeps fp32 master
+ * copies, Adam moments and every buffer of the backward pass (46 more planes of 16 bytes per voxel:
+ * the stored activations and the gradient planes).
+ * gell_surrogate_train_pair: one pair of the running model.  The plain solver advances the field by
+ * `substeps` (the target); the operator runs from the field before them; the loss is the mean of
+ * ((q - target) / b)^2 inside the boundary layers.  Its gradient goes back through the ten layers:
+ * data gradients on the tensor cores; weight gradients on the tensor cores for the 32 -> 32
+ * layers, on the CUDA cores for the first and last. Adam (0.9, 0.999, 1e-8) takes a step of rate
+ * `lr` on the gradient clipped to global norm 1.  The field is left at the target.  *loss (if not
+ * NULL) gets the loss before the step (synchronises).
+ * gell_surrogate_train_read: which 0 = the master weights, 1 = the last gradient (count =
+ * gell_surrogate_weight_count()), 2 = the last target field (count = pitched field floats). */
+gell_status gell_surrogate_train_init(gell_ctx* ctx, int substrate, const float* weights, long long count, int substeps,
+                                      float rate_scale);
+gell_status gell_surrogate_train_pair(gell_ctx* ctx, int substrate, float lr, float* loss);
+gell_status gell_surrogate_train_read(gell_ctx* ctx, int substrate, int which, float* host, long long count);
 long long gell_surrogate_weight_count(void);
 gell_status gell_surrogate_load(gell_ctx* ctx, int substrate, const float* weights, long long count, int substeps,
                                 float rate_scale, float threshold);
