@@ -256,6 +256,30 @@ def time_inference(N: int = 128, reps: int = 3, ring: bool = True, path: str | N
     return out
 
 
+def time_training(N: int = 128, reps: int = 2, cells: int = 40_000, log=print) -> dict:
+    """Per-kernel device times of `reps` training pairs (gell_surrogate_train_pair) on an N^3 grid
+    holding a quasi-steady spheroid of `cells` cells, starting from the packaged weights."""
+    import gell_b200 as gb
+
+    sw = load_weights(DEFAULT_WEIGHTS)
+    c = gb.lattice_spheroid(cells, N * 10.0 / 2, 5, 10.0, N)
+    with gb.Simulation(voxel_num=N, voxel_length=10.0, max_cell_num=cells) as sim:
+        sim.add_substrate(gb.oxygen())
+        sim.import_cells(c)
+        sim.PreLOD()
+        sim.LODsolver(100, 0)
+        sim.surrogate_train_init(0, sw.weights, sw.substeps, sw.rate_scale)
+        sim.surrogate_train_pair(0, 1e-5)  # first launches (module loading) outside the timing
+        sim.profile(True)
+        sim.profile_read(reset=True)
+        for _ in range(reps):
+            sim.surrogate_train_pair(0, 1e-5, want_loss=False)
+        prof = sim.profile_read(reset=True)
+    out = {k: {"launches": v[0] / reps, "ms_per_pair": v[1] / reps} for k, v in prof.items()}
+    log(out)
+    return out
+
+
 def main(argv=None) -> int:
     import argparse
     import sys
@@ -271,11 +295,19 @@ def main(argv=None) -> int:
         t = tp.parse_args(argv[1:])
         time_inference(t.N, t.reps, not t.no_ring, t.weights)
         return 0
+    if argv and argv[0] == "time-train":
+        tp = argparse.ArgumentParser(description="Time the training kernels on an N^3 grid.")
+        tp.add_argument("--N", type=int, default=128)
+        tp.add_argument("--reps", type=int, default=2)
+        t = tp.parse_args(argv[1:])
+        time_training(t.N, t.reps)
+        return 0
     if argv and argv[0] == "fit":
         argv = argv[1:]
     ap = argparse.ArgumentParser(description="Fit the LOD surrogate of oxygen and calibrate its judge "
                                              "(`python -m gell_b200.surrogate [fit] --out FILE`; "
-                                             "`... time --N 128` times the operator's kernels).")
+                                             "`... time --N 128` times the operator's kernels, "
+                                             "`... time-train --N 128` those of a training pair).")
     ap.add_argument("--out", required=True)
     ap.add_argument("--N", type=int, default=256)
     ap.add_argument("--pairs", type=int, default=2000)
