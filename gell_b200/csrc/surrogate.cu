@@ -653,12 +653,16 @@ __global__ void __launch_bounds__(192, 1) k_wgrad(const __grid_constant__ WgradA
 // line's voxels and over every line the block visits; each block writes its partial sums.
 constexpr int kThinMaxW = 16;
 
+// Staged runs are kept channel-major, xs[e][r][x] with a row pitch of 3 mod 32 words, so that the
+// 27 taps a warp reads at one x fall in 27 different banks.
+__host__ __device__ inline int thin_pitch(int N) { return (N + 2 - 3 + 31) / 32 * 32 + 3; }
+
 __global__ void k_wgrad_thin(const uint4* X, int cin, const uint4* G, int cout, int N, long long nvox,
                              float* partial) {
     extern __shared__ float sm[];
-    const int RUN = N + 2;
-    float* xs = sm;                // [9][RUN][8]
-    float* gs = sm + 9 * RUN * 8;  // [N][cout]
+    const int RUN = N + 2, RP = thin_pitch(N);
+    float* xs = sm;                // [8][9][RP]
+    float* gs = sm + 8 * 9 * RP;   // [N][cout]
     const int total = cout * cin * 27;
     float acc[kThinMaxW];
 #pragma unroll
@@ -688,8 +692,8 @@ __global__ void k_wgrad_thin(const uint4* X, int cin, const uint4* G, int cout, 
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const float2 f = unpack_bf16(w4[j]);
-                    xs[i * 8 + 2 * j] = f.x;
-                    xs[i * 8 + 2 * j + 1] = f.y;
+                    xs[((2 * j) * 9 + r) * RP + xi] = f.x;
+                    xs[((2 * j + 1) * 9 + r) * RP + xi] = f.y;
                 }
             }
             __syncthreads();
@@ -700,9 +704,9 @@ __global__ void k_wgrad_thin(const uint4* X, int cin, const uint4* G, int cout, 
                     const int co = w / (cin * 27), ci = (w / 27) % cin, tap = w % 27;
                     if (ci / 8 == pl) {
                         const int r = tap / 3, dx = tap % 3;
-                        const float* xr = xs + (r * RUN + dx) * 8 + (ci % 8);
+                        const float* xr = xs + ((ci % 8) * 9 + r) * RP + dx;
                         float sacc = 0.f;
-                        for (int x = 0; x < N; ++x) sacc = __fmaf_rn(xr[x * 8], gs[x * cout + co], sacc);
+                        for (int x = 0; x < N; ++x) sacc = __fmaf_rn(xr[x], gs[x * cout + co], sacc);
                         acc[j] += sacc;
                     }
                 }
@@ -1127,7 +1131,7 @@ static gell_status wgrad_layer(gell_ctx* c, SurrogateState* S, int l, const CUte
         GELL_KERNEL(c, "k_sum_partials", (k_sum_partials<<<(nw + 255) / 256, 256, 0, c->stream>>>(T->partial, grid, nw, nw,
                                                                                                   T->grad + T->off_w[l])));
     } else {
-        const int smem = (9 * (N + 2) * 8 + N * sh.cout) * 4;
+        const int smem = (8 * 9 * thin_pitch(N) + N * sh.cout) * 4;
         GELL_CUDA(c, cudaFuncSetAttribute(k_wgrad_thin, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         GELL_KERNEL(c, "k_wgrad_thin", (k_wgrad_thin<<<thin_blocks(), 256, smem, c->stream>>>(X, sh.cin, G, sh.cout, N,
                                                                                                 c->nvox, T->partial)));
