@@ -322,7 +322,7 @@ gell_status gell_sync(gell_ctx* c) {
     GELL_CUDA(c, cudaMemcpy(&herr, c->dev_err, 4, cudaMemcpyDeviceToHost));
     if (herr) {
         // reported once: the word is cleared so that the context can go on
-        GELL_CUDA(c, cudaMemset(c->dev_err, 0, 4));
+        GELL_CUDA(c, cudaMemsetAsync(c->dev_err, 0, 4, c->stream));  // ordered before the next kernels
         return fail(c, GELL_ERR_TIMEOUT, "a bounded device wait gave up (code " + std::to_string(herr) + ")");
     }
     return GELL_OK;
@@ -438,7 +438,9 @@ gell_status gell_substrate_add(gell_ctx* c, const gell_substrate* s, int* index_
         efr[c->g.N + i] = sub.F[i];
         efr[2 * c->g.N + i] = recip_rn(sub.F[i]);
     }
-    GELL_CUDA(c, cudaMemcpy(sub.EF, efr.data(), efr.size() * 4, cudaMemcpyHostToDevice));
+    // stream-ordered uploads (the context's stream is non-blocking, so a plain cudaMemcpy would not
+    // be ordered before the sweeps that read these), finished before the host vectors go away
+    GELL_CUDA(c, cudaMemcpyAsync(sub.EF, efr.data(), efr.size() * 4, cudaMemcpyHostToDevice, c->stream));
     {
         const int Na = (c->g.N + 31) / 32 * 32;
         std::vector<float4> frs((size_t)Na);
@@ -456,7 +458,9 @@ gell_status gell_substrate_add(gell_ctx* c, const gell_substrate* s, int* index_
         }
         sub.conv_R = recip_rn(sub.F[N - 2]);
         GELL_CUDA(c, cudaMalloc(&sub.FRS, frs.size() * sizeof(float4)));
-        GELL_CUDA(c, cudaMemcpy(sub.FRS, frs.data(), frs.size() * sizeof(float4), cudaMemcpyHostToDevice));
+        GELL_CUDA(c, cudaMemcpyAsync(sub.FRS, frs.data(), frs.size() * sizeof(float4), cudaMemcpyHostToDevice,
+                                     c->stream));
+        GELL_CUDA(c, cudaStreamSynchronize(c->stream));
     }
     GELL_KERNEL(c, "k_fill", k_fill<<<blocks_for(c->nvox_p, 256), 256, 0, c->stream>>>(sub.p, c->nvox_p, s->init));
     GELL_CUDA(c, cudaMemsetAsync(sub.rate, 0, fb, c->stream));

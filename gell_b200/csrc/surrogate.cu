@@ -1265,8 +1265,11 @@ gell_status gell_surrogate_load(gell_ctx* c, int sub, const float* weights, long
             if (cudaMalloc(&S->w[l], img.size() * 2) != cudaSuccess || cudaMalloc(&S->bias[l], bias.size() * 4) != cudaSuccess)
                 return fail(c, GELL_ERR_ALLOC, "surrogate weights");
         }
-        GELL_CUDA(c, cudaMemcpy(S->w[l], img.data(), img.size() * 2, cudaMemcpyHostToDevice));
-        GELL_CUDA(c, cudaMemcpy(S->bias[l], bias.data(), bias.size() * 4, cudaMemcpyHostToDevice));
+        // copies on the context's stream (a non-blocking stream: a plain cudaMemcpy would not be
+        // ordered before the kernels that read these buffers), finished before the vectors go away
+        GELL_CUDA(c, cudaMemcpyAsync(S->w[l], img.data(), img.size() * 2, cudaMemcpyHostToDevice, c->stream));
+        GELL_CUDA(c, cudaMemcpyAsync(S->bias[l], bias.data(), bias.size() * 4, cudaMemcpyHostToDevice, c->stream));
+        GELL_CUDA(c, cudaStreamSynchronize(c->stream));
     }
     c->sur[sub] = S;
     if (fresh) {
@@ -1276,7 +1279,7 @@ gell_status gell_surrogate_load(gell_ctx* c, int sub, const float* weights, long
             cudaMalloc(&S->backup, field) != cudaSuccess || cudaMalloc(&S->dmax, 4) != cudaSuccess ||
             cudaMallocHost(&S->hmax, 4) != cudaSuccess)
             return fail(c, GELL_ERR_ALLOC, "surrogate activations (10 planes of 16 bytes per voxel)");
-        GELL_CUDA(c, cudaMemset(S->in, 0, 2 * plane));
+        GELL_CUDA(c, cudaMemsetAsync(S->in, 0, 2 * plane, c->stream));
         gell_status st = plane_map(c, &S->map_in, S->in, 2);
         if (st == GELL_OK) st = plane_map(c, &S->map_h, S->h, 4);
         if (st == GELL_OK) st = plane_map(c, &S->map_t, S->t, 4);
@@ -1360,8 +1363,8 @@ gell_status gell_surrogate_train_init(gell_ctx* c, int sub, const float* weights
         for (int l = 1; ok && l < kLayers; ++l)
             ok = cudaMalloc(&T->wt[l], (size_t)27 * (dgrad_cin8(l) / 2) * 2 * dgrad_nout(l) * 8 * 2) == cudaSuccess;
         if (!ok) return fail(c, GELL_ERR_ALLOC, "surrogate training buffers (46 planes of 16 bytes per voxel)");
-        GELL_CUDA(c, cudaMemset(T->zero_bias, 0, 32 * 4));
-        GELL_CUDA(c, cudaMemset(T->gd, 0, 2 * plane));
+        GELL_CUDA(c, cudaMemsetAsync(T->zero_bias, 0, 32 * 4, c->stream));
+        GELL_CUDA(c, cudaMemsetAsync(T->gd, 0, 2 * plane, c->stream));
         for (int k = 0; k < 5 && st == GELL_OK; ++k) st = plane_map(c, &T->mh[k], T->hb[k], 4);
         for (int k = 0; k < 4 && st == GELL_OK; ++k) st = plane_map(c, &T->mt[k], T->tb[k], 4);
         if (st == GELL_OK) st = plane_map(c, &T->mgd, T->gd, 2);
@@ -1373,10 +1376,12 @@ gell_status gell_surrogate_train_init(gell_ctx* c, int sub, const float* weights
     }
     TrainState* T = S->train;
     T->step = 0;
-    GELL_CUDA(c, cudaMemcpy(T->master, weights, count * 4, cudaMemcpyHostToDevice));
-    GELL_CUDA(c, cudaMemset(T->m, 0, count * 4));
-    GELL_CUDA(c, cudaMemset(T->v, 0, count * 4));
-    return repack(c, S);
+    GELL_CUDA(c, cudaMemcpyAsync(T->master, weights, count * 4, cudaMemcpyHostToDevice, c->stream));
+    GELL_CUDA(c, cudaMemsetAsync(T->m, 0, count * 4, c->stream));
+    GELL_CUDA(c, cudaMemsetAsync(T->v, 0, count * 4, c->stream));
+    if ((st = repack(c, S)) != GELL_OK) return st;
+    GELL_CUDA(c, cudaStreamSynchronize(c->stream));  // `weights` may go away after the return
+    return GELL_OK;
 }
 
 gell_status gell_surrogate_train_pair(gell_ctx* c, int sub, float lr, float* loss) {
