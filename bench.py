@@ -473,7 +473,6 @@ def run_c5(args, rank, world, local_rank):
     sim.PreLOD()
     sim.LODsolver(C5_WARM, 0)  # from the boundary value to a quasi-steady field
     sim.set_conv_ring(not args.no_conv_ring)
-    sim.set_conv_wide(args.conv_wide)
     sim.surrogate_load(0, sw.weights, K, sw.rate_scale, sw.threshold)
     b = float(gb.oxygen().boundary)
     inner = ~gs.shell_mask(C5_N)
@@ -540,7 +539,7 @@ def run_c5(args, rank, world, local_rank):
         "data": "synthetic: seeded jittered-lattice spheroid of 300,000 cells; weights fitted on 2,000 pairs from the "
                 "plain solver (gell_b200.surrogate)",
         "config": {"workload": C5_WORKLOAD, "voxels": C5_N ** 3, "substeps_per_block": K,
-                   "conv_ring": not args.no_conv_ring, "conv_wide": bool(args.conv_wide),
+                   "conv_ring": not args.no_conv_ring,
                    "warm_substeps": C5_WARM, "judge_threshold": sw.threshold, "l2": "each field is 67 MB; the "
                    "operator's activations are 1.07 GB per 32-channel tensor"},
         "plain": {"value": K / (tp / 1e3), "ms_per_block": tp},
@@ -730,7 +729,6 @@ def main():
                          "against the plain solver at 256^3")
     ap.add_argument("--surrogate-weights", default=None, help="c5: weight file (default: the packaged one)")
     ap.add_argument("--no-conv-ring", action="store_true", help="c5: convolutions without the row ring")
-    ap.add_argument("--conv-wide", action="store_true", help="c5: convolutions with the weights as the A operand")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -388,10 +388,6 @@ class Simulation:
         """The surrogate's convolutions with (default) or without the row ring along y."""
         self._check(self.lib.gell_set_option(self.h, 4, int(bool(on))), "gell_set_option")
 
-    def set_conv_wide(self, on: bool = True) -> None:
-        """The surrogate's convolutions with the weights as the MMA's A operand (GELL_OPT_CONV_WIDE)."""
-        self._check(self.lib.gell_set_option(self.h, 5, int(bool(on))), "gell_set_option")
-
     def launch_count(self) -> int:
         v = ctypes.c_int64()
         self._check(self.lib.gell_launch_count(self.h, ctypes.byref(v)), "gell_launch_count")

@@ -115,7 +115,6 @@ struct gell_ctx {
     std::vector<gell::Substrate> subs;
     gell::SurrogateState* sur[8] = {};  // per substrate, created by gell_surrogate_load
     bool conv_ring = true;              // GELL_OPT_CONV_RING: the surrogate's convolutions reuse rows along y
-    bool conv_wide = false;             // GELL_OPT_CONV_WIDE: weights as the MMA's A operand, N = 144 voxels
     bool rate_valid = false;
     bool exact_chain = false;  // GELL_OPT_EXACT_CHAIN
     int sweep_warps = 0;       // GELL_OPT_SWEEP_WARPS (0: as many as shared memory allows)

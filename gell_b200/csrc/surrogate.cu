@@ -516,279 +516,6 @@ __global__ void __launch_bounds__(192, 1) k_conv3_ring(const __grid_constant__ C
     }
 }
 
-// ---------------------------------------------------------------- k_conv3_wide
-// The same convolution with the roles of the operands swapped, so that each MMA is 4.5x wider:
-// A = the weights of one input row (dy, dz) and 16 input channels, M = 128 rows (dx, co) (96 used);
-// B = a staged run of 144 voxels x0-1 .. x0+142 of that row (N = 144, K-major: the 8-channel planes
-// as they are); D[(dx, co)][j] = sum over rows and channels of W[co][ci][row, dx] X[ci][x0 - 1 + j].
-// A tile of 128 outputs is 9 rows x (input planes / 2) MMAs; the output is
-// out[co][x0 + i] = sum_dx D[(dx, co)][i + dx], formed by the epilogue: warps dx = 0..2 read 34
-// columns of their 32 lanes per chunk of 32 outputs into shared memory, then each of the 128
-// epilogue threads sums one (voxel, 8-channel plane) over dx and stores 16 bytes.  Rows come
-// through the same y ring as k_conv3_ring (5 group slots).  Accumulators at TMEM columns 0 and 256.
-constexpr int kWN = 144;                 // B columns (staged voxels)
-constexpr int kWRunPlaneB = kWN * 16;    // 2304
-constexpr int kWRing = 5;
-constexpr int kWBufPitch = 36;           // floats per (dx, column) row of the exchange buffer
-
-template <int CIN8>
-struct WideSmem {
-    static constexpr int kRunB = CIN8 * kWRunPlaneB;
-    static constexpr int kGroupB = 3 * kRunB;
-    static constexpr int kHalves = CIN8 / 2;
-    static constexpr int kATile = 128 * 32;              // one (row, half) weight tile, bytes
-    static constexpr int kWB = 9 * kHalves * kATile;
-    static constexpr int kBufB = 3 * 34 * kWBufPitch * 4;
-    static constexpr int kBars = kWRing * kGroupB + kWB + kBufB;
-    static constexpr int kBytes = kBars + (2 * kWRing + 6) * 8 + 16;
-};
-
-__device__ __forceinline__ void tmem_ld2(uint32_t a, uint32_t (&v)[2]) {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0,%1}, [%2];" : "=r"(v[0]), "=r"(v[1]) : "r"(a));
-}
-__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
-
-// One (voxel, plane) output of the wide kernel: f[8] = the eight channels' sums; MODE as store_tile.
-template <int MODE>
-__device__ __forceinline__ void store_plane(const ConvArgs& a, float (&f)[8], int pl, int x, int y, int z) {
-    if constexpr (MODE == kField) {
-        const long long pi = (long long)x + (long long)a.P * y + a.PN * z;
-        const int N = a.N;
-        const bool shell = x < 2 || x > N - 3 || y < 2 || y > N - 3 || z < 2 || z > N - 3;
-        a.field_out[pi] = shell ? a.bval : __fmaf_rn(a.scale, f[0], a.field_in[pi]);
-    } else {
-        const long long vox = (long long)x + (long long)a.N * (y + (long long)a.N * z);
-        if constexpr (MODE == kResidual || MODE == kResMask) {
-            const uint4 r = a.res[pl * a.nvox + vox];
-            const uint32_t rr[4] = {r.x, r.y, r.z, r.w};
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const float2 u = unpack_bf16(rr[j]);
-                f[2 * j] += u.x;
-                f[2 * j + 1] += u.y;
-            }
-        }
-        if constexpr (MODE == kMask || MODE == kResMask) {
-            const uint4 m = a.aux[pl * a.nvox + vox];
-            const uint32_t mm[4] = {m.x, m.y, m.z, m.w};
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const float2 u = unpack_bf16(mm[j]);
-                if (!(u.x > 0.f)) f[2 * j] = 0.f;
-                if (!(u.y > 0.f)) f[2 * j + 1] = 0.f;
-            }
-        }
-        if constexpr (MODE == kRelu) {
-#pragma unroll
-            for (int j = 0; j < 8; ++j) f[j] = fmaxf(f[j], 0.f);
-        }
-        a.out[pl * a.nvox + vox] = make_uint4(pack_bf16(f[0], f[1]), pack_bf16(f[2], f[3]), pack_bf16(f[4], f[5]),
-                                              pack_bf16(f[6], f[7]));
-    }
-}
-
-// COUT: output channels (32, or 1 for the field); CIN8: input planes.
-template <int CIN8, int COUT, int MODE>
-__global__ void __launch_bounds__(192, 1) k_conv3_wide(const __grid_constant__ ConvArgs a) {
-    using L = WideSmem<CIN8>;
-    extern __shared__ __align__(1024) uint8_t smem[];
-    uint8_t* wsm = smem + kWRing * L::kGroupB;
-    float* buf = reinterpret_cast<float*>(wsm + L::kWB);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L::kBars);
-    uint64_t* full = bars;
-    uint64_t* empty = bars + kWRing;
-    uint64_t* accf = bars + 2 * kWRing;
-    uint64_t* acce = accf + 2;
-    uint64_t* wbar = acce + 2;
-    uint64_t* done = wbar + 1;
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-
-    if (threadIdx.x == 0) {
-        for (int i = 0; i < kWRing; ++i) {
-            mbar_init(&full[i], 1);
-            mbar_init(&empty[i], 1);
-        }
-        for (int i = 0; i < 2; ++i) {
-            mbar_init(&accf[i], 1);
-            mbar_init(&acce[i], 4);
-        }
-        mbar_init(wbar, 1);
-        mbar_init(done, 1);
-        fence_mbar_init();
-    }
-    if (warp == 1) tmem_alloc(tslot, 512);
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    const uint32_t tmem = *tslot;
-    const int nyc = (a.N + kUnitY - 1) / kUnitY;
-    const long long U = (long long)a.tiles_x * nyc * a.N;
-
-    if (warp == 0) {
-        if (lane == 0) {
-            mbar_arrive_expect(wbar, (uint32_t)L::kWB);
-            for (int off = 0; off < L::kWB; off += 16384) {
-                const int nb = L::kWB - off < 16384 ? L::kWB - off : 16384;
-                bulk_load(wsm + off, a.w + off, (uint32_t)nb, wbar);
-            }
-            bool ok = true;
-            int g = 0;
-            for (long long u = blockIdx.x; ok && u < U; u += gridDim.x) {
-                int x0, y0, y1, z;
-                unit_of(a, u, x0, y0, y1, z);
-                for (int yy = y0 - 1; yy <= y1; ++yy, ++g) {
-                    const int sl = g % kWRing;
-                    if (g >= kWRing && !mbar_wait1(&empty[sl], ((g / kWRing) - 1) & 1, a.err, 41)) {
-                        ok = false;
-                        break;
-                    }
-                    uint8_t* gb = smem + sl * L::kGroupB;
-                    mbar_arrive_expect(&full[sl], (uint32_t)(3 * L::kRunB));
-                    for (int dz = 0; dz < 3; ++dz)
-                        tma_load_5d(gb + dz * L::kRunB, &a.in, 0, x0 - 1, yy, z + dz - 1, 0, &full[sl]);
-                }
-            }
-        }
-    } else if (warp == 1) {
-        if (lane == 0) {
-            constexpr uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kWN >> 3) << 17) |
-                                       ((uint32_t)(128 >> 4) << 24);
-            bool ok = mbar_wait1(wbar, 0, a.err, 42);
-            const uint64_t a0 = sdesc(smem_u32(wsm), 128 * 16, 128);
-            const uint32_t rbase = smem_u32(smem);
-            int g = 0, k = 0;
-            for (long long u = blockIdx.x; ok && u < U; u += gridDim.x) {
-                int x0, y0, y1, z;
-                unit_of(a, u, x0, y0, y1, z);
-                const int ny = y1 - y0;
-                for (int i = 0; i < ny; ++i, ++k) {
-                    const int ac = k & 1;
-                    for (int j = 0; j < 3 && ok; ++j) {
-                        const int gg = g + i + j;
-                        ok = mbar_wait1(&full[gg % kWRing], (gg / kWRing) & 1, a.err, 43);
-                    }
-                    if (ok && k >= 2) ok = mbar_wait1(&acce[ac], ((k >> 1) - 1) & 1, a.err, 44);
-                    if (!ok) break;
-                    tc_fence_after();
-                    const uint32_t d = tmem + (uint32_t)(ac * 256);
-                    uint64_t gb[3];
-#pragma unroll
-                    for (int j = 0; j < 3; ++j)
-                        gb[j] = sdesc(rbase + (uint32_t)(((g + i + j) % kWRing) * L::kGroupB), kWRunPlaneB, 128);
-#pragma unroll
-                    for (int r = 0; r < 9; ++r) {
-#pragma unroll
-                        for (int h = 0; h < L::kHalves; ++h) {
-                            const uint32_t ao = ((r * L::kHalves + h) * L::kATile) >> 4;
-                            const uint32_t bo = ((r / 3) * L::kRunB + 2 * h * kWRunPlaneB) >> 4;
-                            mma_bf16(d, a0 + ao, gb[r % 3] + bo, idesc, (r | h) != 0 ? 1u : 0u);
-                        }
-                    }
-                    mma_commit(&accf[ac]);
-                    if (i < ny - 1) {
-                        mma_commit(&empty[(g + i) % kWRing]);
-                    } else {
-                        for (int j = 0; j < 3; ++j) mma_commit(&empty[(g + i + j) % kWRing]);
-                    }
-                }
-                g += ny + 2;
-            }
-            mma_commit(done);
-            mbar_wait1(done, 0, a.err, 45);
-        }
-    } else {
-        const int q = warp & 3;              // TMEM lanes 32q..: dx = q (q = 3: padding rows)
-        const int e = threadIdx.x - 64;      // 0..127: output voxel t = e & 31, plane pl = e >> 5
-        const int t = e & 31, pl = e >> 5;
-        float bias[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) bias[j] = (8 * pl + j < COUT) ? a.bias[8 * pl + j] : 0.f;
-        int k = 0;
-        bool ok = true;
-        for (long long u = blockIdx.x; ok && u < U; u += gridDim.x) {
-            int x0, y0, y1, z;
-            unit_of(a, u, x0, y0, y1, z);
-            for (int y = y0; y < y1; ++y, ++k) {
-                const int ac = k & 1;
-                if (!mbar_wait(&accf[ac], (k >> 1) & 1, a.err, 46)) {
-                    ok = false;
-                    break;
-                }
-                tc_fence_after();
-#pragma unroll 1
-                for (int c = 0; c < 4; ++c) {
-                    const int c0 = 32 * c;
-                    if (q < 3) {
-                        uint32_t v[32], w[2];
-                        const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(ac * 256 + c0);
-                        tmem_ld32(ta, v);
-                        tmem_ld2(ta + 32, w);
-                        tmem_wait_ld();
-                        if (c == 3) {
-                            tc_fence_before();
-                            __syncwarp();
-                            if (lane == 0) mbar_arrive(&acce[ac]);
-                        }
-                        float* bq = buf + (size_t)q * 34 * kWBufPitch + lane;
-#pragma unroll
-                        for (int j = 0; j < 32; ++j) bq[j * kWBufPitch] = __uint_as_float(v[j]);
-                        bq[32 * kWBufPitch] = __uint_as_float(w[0]);
-                        bq[33 * kWBufPitch] = __uint_as_float(w[1]);
-                    } else if (c == 3 && lane == 0) {
-                        mbar_arrive(&acce[ac]);
-                    }
-                    epi_bar();
-                    const int x = x0 + c0 + t;
-                    if (x < a.N && (MODE != kField || pl == 0) && 8 * pl < COUT) {
-                        float f[8];
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) f[j] = bias[j];
-#pragma unroll
-                        for (int dx = 0; dx < 3; ++dx) {
-                            const float4* src =
-                                reinterpret_cast<const float4*>(buf + ((size_t)dx * 34 + t + dx) * kWBufPitch + 8 * pl);
-                            const float4 u0 = src[0], u1 = src[1];
-                            f[0] += u0.x; f[1] += u0.y; f[2] += u0.z; f[3] += u0.w;
-                            f[4] += u1.x; f[5] += u1.y; f[6] += u1.z; f[7] += u1.w;
-                        }
-                        store_plane<MODE>(a, f, pl, x, y, z);
-                    }
-                    epi_bar();
-                }
-            }
-        }
-    }
-    tc_fence_before();
-    __syncthreads();
-    if (warp == 1) {
-        __syncwarp();
-        tc_fence_after();
-        tmem_dealloc(tmem, 512);
-    }
-}
-
-// Weights of the wide kernel from the fp32 master weights W[cout][cin][27] of one layer: tile (row
-// r = 3 kz + ky, half h) = [kc][m][8], row m = 32 dx + n (dx < 3), input channel 16h + 8kc + e;
-// `transpose` as k_pack_w (the data-gradient convolution: channels swapped, taps mirrored).
-__global__ void k_pack_wide(const float* W, int cin, int cout, int cin8, int transpose, __nv_bfloat16* img) {
-    const int halves = cin8 / 2;
-    const int n_img = 9 * halves * 2 * 128 * 8;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_img; i += gridDim.x * blockDim.x) {
-        const int e = i % 8, m = (i / 8) % 128, kc = (i / 1024) % 2, h = (i / 2048) % halves, r = i / (2048 * halves);
-        const int dx = m / 32, n = m % 32, k = 16 * h + 8 * kc + e, tap = 3 * r + dx;
-        float v = 0.f;
-        if (dx < 3) {
-            if (!transpose) {
-                if (n < cout && k < cin) v = W[((size_t)n * cin + k) * 27 + tap];
-            } else {
-                if (k < cout && n < cin) v = W[((size_t)k * cin + n) * 27 + (26 - tap)];
-            }
-        }
-        img[i] = __float2bfloat16_rn(v);
-    }
-}
-
 // ---------------------------------------------------------------- weight gradients
 // k_wgrad (32 -> 32 layers, tcgen05): dW[co][ci][tap] = sum over voxels v of X[ci, v + tap] * G[co, v]
 // (X = the layer's input, G = the gradient of its output, zero outside the grid).  The voxels are
@@ -1187,8 +914,6 @@ struct TrainState {
     float* scal = nullptr;       // [0] gradient sum of squares, [1] loss, [2..] loss partials
     float* hloss = nullptr;      // pinned
     uint8_t* wt[kLayers] = {};   // data-gradient images (layers 1..9)
-    uint8_t* wwt[kLayers] = {};  // the same for k_conv3_wide
-    CUtensorMap mh_w[5], mt_w[4], mgd_w, mgh_w, mgu_w;  // 144-voxel boxes for k_conv3_wide
     uint4* hb[5] = {};
     uint4* tb[4] = {};
     uint4 *gh = nullptr, *gu = nullptr, *gd = nullptr;
@@ -1201,7 +926,6 @@ struct SurrogateState {
     int substeps = 0;
     float rate_scale = 0.f, threshold = 0.f;
     uint8_t* w[kLayers] = {};   // packed weight images
-    uint8_t* ww[kLayers] = {};  // the same for k_conv3_wide
     float* bias[kLayers] = {};  // padded to the layer's NOUT
     uint4* in = nullptr;        // 2 planes
     uint4* h = nullptr;         // 4 planes
@@ -1211,7 +935,6 @@ struct SurrogateState {
     unsigned* dmax = nullptr;   // judge scratch
     unsigned* hmax = nullptr;   // pinned host copy
     CUtensorMap map_in, map_h, map_t;
-    CUtensorMap map_in_w, map_h_w, map_t_w;  // 144-voxel boxes for k_conv3_wide
     double conv_flops = 0;      // algorithmic FLOPs of one inference (real channels only)
     struct TrainState* train = nullptr;
 };
@@ -1221,7 +944,6 @@ void surrogate_free(gell_ctx* c) {
         if (!s) continue;
         for (int l = 0; l < kLayers; ++l) {
             if (s->w[l]) cudaFree(s->w[l]);
-            if (s->ww[l]) cudaFree(s->ww[l]);
             if (s->bias[l]) cudaFree(s->bias[l]);
         }
         for (void* p : {(void*)s->in, (void*)s->h, (void*)s->t, (void*)s->ph, (void*)s->backup, (void*)s->dmax})
@@ -1232,7 +954,6 @@ void surrogate_free(gell_ctx* c) {
                             (void*)t->zero_bias, (void*)t->scal, (void*)t->gh, (void*)t->gu, (void*)t->gd, (void*)t->tgt})
                 if (p) cudaFree(p);
             for (auto* p : t->wt) if (p) cudaFree(p);
-            for (auto* p : t->wwt) if (p) cudaFree(p);
             for (auto* p : t->hb) if (p) cudaFree(p);
             for (auto* p : t->tb) if (p) cudaFree(p);
             if (t->hloss) cudaFreeHost(t->hloss);
@@ -1291,16 +1012,21 @@ static void pack_layer(const float* W, const LayerShape& s, std::vector<uint16_t
 }
 
 template <int CIN8, int NOUT, int MODE>
-static gell_status launch_conv(gell_ctx* c, const char* name, const CUtensorMap& in, const CUtensorMap& in_w,
-                               const uint8_t* w, const uint8_t* ww, const float* bias, uint4* out, const uint4* res,
-                               const uint4* aux, float* fout, const float* fin, float scale, float bval) {
+static gell_status launch_conv(gell_ctx* c, const char* name, const CUtensorMap& in, const uint8_t* w, const float* bias,
+                               uint4* out, const uint4* res, const uint4* aux, float* fout, const float* fin, float scale,
+                               float bval) {
     using L = ConvSmem<CIN8, NOUT>;
     using R = RingSmem<CIN8, NOUT>;
-    constexpr int COUT = MODE == kField ? 1 : 32;
-    using W = WideSmem<CIN8>;
+    // the shared-memory opt-in is a per-device attribute; setting it is cheap, so every launch does
+    if (c->conv_ring)
+        GELL_CUDA(c, cudaFuncSetAttribute(k_conv3_ring<CIN8, NOUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          R::kBytes));
+    else
+        GELL_CUDA(c, cudaFuncSetAttribute(k_conv3<CIN8, NOUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          L::kBytes));
     ConvArgs a{};
-    a.in = c->conv_wide ? in_w : in;
-    a.w = c->conv_wide ? ww : w;
+    a.in = in;
+    a.w = w;
     a.bias = bias;
     a.out = out;
     a.res = res;
@@ -1318,21 +1044,11 @@ static gell_status launch_conv(gell_ctx* c, const char* name, const CUtensorMap&
     a.err = c->dev_err;
     int sms = 0;
     GELL_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-    const long long units = (long long)a.tiles_x * ((c->g.N + kUnitY - 1) / kUnitY) * c->g.N;
-    // the shared-memory opt-in is a per-device attribute; setting it is cheap, so every launch does
-    if (c->conv_wide) {
-        GELL_CUDA(c, cudaFuncSetAttribute(k_conv3_wide<CIN8, COUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          W::kBytes));
-        const int grid = (int)(units < sms ? units : sms);
-        GELL_KERNEL(c, name, (k_conv3_wide<CIN8, COUT, MODE><<<grid, 192, W::kBytes, c->stream>>>(a)));
-    } else if (c->conv_ring) {
-        GELL_CUDA(c, cudaFuncSetAttribute(k_conv3_ring<CIN8, NOUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          R::kBytes));
+    if (c->conv_ring) {
+        const long long units = (long long)a.tiles_x * ((c->g.N + kUnitY - 1) / kUnitY) * c->g.N;
         const int grid = (int)(units < sms ? units : sms);
         GELL_KERNEL(c, name, (k_conv3_ring<CIN8, NOUT, MODE><<<grid, 192, R::kBytes, c->stream>>>(a)));
     } else {
-        GELL_CUDA(c, cudaFuncSetAttribute(k_conv3<CIN8, NOUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          L::kBytes));
         const int grid = (int)(a.tiles < sms ? a.tiles : sms);
         GELL_KERNEL(c, name, (k_conv3<CIN8, NOUT, MODE><<<grid, 192, L::kBytes, c->stream>>>(a)));
     }
@@ -1354,20 +1070,15 @@ static gell_status run_layers(gell_ctx* c, int sub, SurrogateState* S, int layer
     gell_status st = GELL_OK;
     for (int l = 0; l < layers && st == GELL_OK; ++l) {
         const uint8_t* w = S->w[l];
-        const uint8_t* ww = S->ww[l];
         const float* bi = S->bias[l];
         if (l == 0)
-            st = launch_conv<2, 32, kRelu>(c, "k_conv3_in", S->map_in, S->map_in_w, w, ww, bi, S->h, nullptr, nullptr,
-                                           nullptr, nullptr, 0.f, 0.f);
+            st = launch_conv<2, 32, kRelu>(c, "k_conv3_in", S->map_in, w, bi, S->h, nullptr, nullptr, nullptr, nullptr, 0.f, 0.f);
         else if (l == kLayers - 1)
-            st = launch_conv<4, 16, kField>(c, "k_conv3_out", S->map_h, S->map_h_w, w, ww, bi, nullptr, nullptr, nullptr,
-                                            S->ph, Su.p, b, b);
+            st = launch_conv<4, 16, kField>(c, "k_conv3_out", S->map_h, w, bi, nullptr, nullptr, nullptr, S->ph, Su.p, b, b);
         else if (l & 1)
-            st = launch_conv<4, 32, kRelu>(c, "k_conv3_hidden", S->map_h, S->map_h_w, w, ww, bi, S->t, nullptr, nullptr,
-                                           nullptr, nullptr, 0.f, 0.f);
+            st = launch_conv<4, 32, kRelu>(c, "k_conv3_hidden", S->map_h, w, bi, S->t, nullptr, nullptr, nullptr, nullptr, 0.f, 0.f);
         else
-            st = launch_conv<4, 32, kResidual>(c, "k_conv3_hidden", S->map_t, S->map_t_w, w, ww, bi, S->h, S->h, nullptr,
-                                               nullptr, nullptr, 0.f, 0.f);
+            st = launch_conv<4, 32, kResidual>(c, "k_conv3_hidden", S->map_t, w, bi, S->h, S->h, nullptr, nullptr, nullptr, 0.f, 0.f);
     }
     return st;
 }
@@ -1385,16 +1096,10 @@ static gell_status repack(gell_ctx* c, SurrogateState* S) {
         GELL_KERNEL(c, "k_pack_w", (k_pack_w<<<64, 256, 0, c->stream>>>(T->master + T->off_w[l], sh.cin, sh.cout, sh.cin8,
                                                                          sh.nout, 0, (__nv_bfloat16*)S->w[l])));
         GELL_KERNEL(c, "k_pack_bias", (k_pack_bias<<<1, 32, 0, c->stream>>>(T->master + T->off_b[l], sh.cout, sh.nout, S->bias[l])));
-        GELL_KERNEL(c, "k_pack_w", (k_pack_wide<<<64, 256, 0, c->stream>>>(T->master + T->off_w[l], sh.cin, sh.cout,
-                                                                            sh.cin8, 0, (__nv_bfloat16*)S->ww[l])));
-        if (l >= 1) {
+        if (l >= 1)
             GELL_KERNEL(c, "k_pack_w", (k_pack_w<<<64, 256, 0, c->stream>>>(T->master + T->off_w[l], sh.cin, sh.cout,
                                                                              dgrad_cin8(l), dgrad_nout(l), 1,
                                                                              (__nv_bfloat16*)T->wt[l])));
-            GELL_KERNEL(c, "k_pack_w", (k_pack_wide<<<64, 256, 0, c->stream>>>(T->master + T->off_w[l], sh.cin,
-                                                                                sh.cout, dgrad_cin8(l), 1,
-                                                                                (__nv_bfloat16*)T->wwt[l])));
-        }
     }
     return GELL_OK;
 }
@@ -1459,19 +1164,18 @@ static gell_status train_pair(gell_ctx* c, int sub, SurrogateState* S, float lr,
     const int pb = blocks_for(c->nvox, 256);
     GELL_KERNEL(c, "k_pack_input", (k_pack_input<<<pb < 148 * 16 ? pb : 148 * 16, 256, 0, c->stream>>>(
                                         Su.p, Su.rate, c->g, 1.f / b, S->rate_scale, S->in)));
-    st = launch_conv<2, 32, kRelu>(c, "k_conv3_in", S->map_in, S->map_in_w, S->w[0], S->ww[0], S->bias[0], T->hb[0],
-                                   nullptr, nullptr, nullptr, nullptr, 0.f, 0.f);
+    st = launch_conv<2, 32, kRelu>(c, "k_conv3_in", S->map_in, S->w[0], S->bias[0], T->hb[0], nullptr, nullptr, nullptr,
+                                   nullptr, 0.f, 0.f);
     for (int k = 0; k < 4 && st == GELL_OK; ++k) {
-        st = launch_conv<4, 32, kRelu>(c, "k_conv3_hidden", T->mh[k], T->mh_w[k], S->w[2 * k + 1], S->ww[2 * k + 1],
-                                       S->bias[2 * k + 1], T->tb[k], nullptr, nullptr, nullptr, nullptr, 0.f, 0.f);
+        st = launch_conv<4, 32, kRelu>(c, "k_conv3_hidden", T->mh[k], S->w[2 * k + 1], S->bias[2 * k + 1], T->tb[k],
+                                       nullptr, nullptr, nullptr, nullptr, 0.f, 0.f);
         if (st == GELL_OK)
-            st = launch_conv<4, 32, kResidual>(c, "k_conv3_hidden", T->mt[k], T->mt_w[k], S->w[2 * k + 2], S->ww[2 * k + 2],
-                                               S->bias[2 * k + 2], T->hb[k + 1], T->hb[k], nullptr, nullptr, nullptr,
-                                               0.f, 0.f);
+            st = launch_conv<4, 32, kResidual>(c, "k_conv3_hidden", T->mt[k], S->w[2 * k + 2], S->bias[2 * k + 2],
+                                               T->hb[k + 1], T->hb[k], nullptr, nullptr, nullptr, 0.f, 0.f);
     }
     if (st == GELL_OK)
-        st = launch_conv<4, 16, kField>(c, "k_conv3_out", T->mh[4], T->mh_w[4], S->w[9], S->ww[9], S->bias[9], nullptr,
-                                        nullptr, nullptr, S->ph, Su.p, b, b);
+        st = launch_conv<4, 16, kField>(c, "k_conv3_out", T->mh[4], S->w[9], S->bias[9], nullptr, nullptr, nullptr, S->ph,
+                                        Su.p, b, b);
     if (st != GELL_OK) return st;
 
     // loss and its gradient
@@ -1483,20 +1187,20 @@ static gell_status train_pair(gell_ctx* c, int sub, SurrogateState* S, float lr,
 
     // backward
     if ((st = wgrad_layer(c, S, 9, nullptr, T->hb[4], nullptr, T->gd, 1)) != GELL_OK) return st;
-    st = launch_conv<2, 32, kLinear>(c, "k_conv3_dgrad", T->mgd, T->mgd_w, T->wt[9], T->wwt[9], T->zero_bias, T->gh,
-                                     nullptr, nullptr, nullptr, nullptr, 0.f, 0.f);
+    st = launch_conv<2, 32, kLinear>(c, "k_conv3_dgrad", T->mgd, T->wt[9], T->zero_bias, T->gh, nullptr, nullptr, nullptr,
+                                     nullptr, 0.f, 0.f);
     for (int k = 3; k >= 0 && st == GELL_OK; --k) {
         if ((st = wgrad_layer(c, S, 2 * k + 2, &T->mt[k], T->tb[k], &T->mgh_g, T->gh, 4)) != GELL_OK) return st;
-        st = launch_conv<4, 32, kMask>(c, "k_conv3_dgrad", T->mgh, T->mgh_w, T->wt[2 * k + 2], T->wwt[2 * k + 2],
-                                       T->zero_bias, T->gu, nullptr, T->tb[k], nullptr, nullptr, 0.f, 0.f);
+        st = launch_conv<4, 32, kMask>(c, "k_conv3_dgrad", T->mgh, T->wt[2 * k + 2], T->zero_bias, T->gu, nullptr,
+                                       T->tb[k], nullptr, nullptr, 0.f, 0.f);
         if (st != GELL_OK) return st;
         if ((st = wgrad_layer(c, S, 2 * k + 1, &T->mh[k], T->hb[k], &T->mgu_g, T->gu, 4)) != GELL_OK) return st;
         if (k > 0)
-            st = launch_conv<4, 32, kResidual>(c, "k_conv3_dgrad", T->mgu, T->mgu_w, T->wt[2 * k + 1], T->wwt[2 * k + 1],
-                                               T->zero_bias, T->gh, T->gh, nullptr, nullptr, nullptr, 0.f, 0.f);
+            st = launch_conv<4, 32, kResidual>(c, "k_conv3_dgrad", T->mgu, T->wt[2 * k + 1], T->zero_bias, T->gh, T->gh,
+                                               nullptr, nullptr, nullptr, 0.f, 0.f);
         else
-            st = launch_conv<4, 32, kResMask>(c, "k_conv3_dgrad", T->mgu, T->mgu_w, T->wt[1], T->wwt[1], T->zero_bias, T->gh,
-                                              T->gh, T->hb[0], nullptr, nullptr, 0.f, 0.f);
+            st = launch_conv<4, 32, kResMask>(c, "k_conv3_dgrad", T->mgu, T->wt[1], T->zero_bias, T->gh, T->gh, T->hb[0],
+                                              nullptr, nullptr, 0.f, 0.f);
     }
     if (st != GELL_OK) return st;
     if ((st = wgrad_layer(c, S, 0, nullptr, S->in, nullptr, T->gh, 4)) != GELL_OK) return st;
@@ -1565,21 +1269,7 @@ gell_status gell_surrogate_load(gell_ctx* c, int sub, const float* weights, long
         // ordered before the kernels that read these buffers), finished before the vectors go away
         GELL_CUDA(c, cudaMemcpyAsync(S->w[l], img.data(), img.size() * 2, cudaMemcpyHostToDevice, c->stream));
         GELL_CUDA(c, cudaMemcpyAsync(S->bias[l], bias.data(), bias.size() * 4, cudaMemcpyHostToDevice, c->stream));
-        // the wide kernel's image, packed on the device from the fp32 weights
-        const size_t wide_b = (size_t)9 * (s.cin8 / 2) * 128 * 32;
-        if (!S->ww[l] && cudaMalloc(&S->ww[l], wide_b) != cudaSuccess) return fail(c, GELL_ERR_ALLOC, "surrogate weights");
-        float* tmp = nullptr;
-        const size_t nW = (size_t)s.cout * s.cin * 27;
-        GELL_CUDA(c, cudaMalloc(&tmp, nW * 4));
-        cudaError_t e = cudaMemcpyAsync(tmp, W - s.cout - nW, nW * 4, cudaMemcpyHostToDevice, c->stream);
-        if (e == cudaSuccess) {
-            k_pack_wide<<<64, 256, 0, c->stream>>>(tmp, s.cin, s.cout, s.cin8, 0, (__nv_bfloat16*)S->ww[l]);
-            c->launches++;
-            e = cudaGetLastError();
-        }
-        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-        cudaFree(tmp);
-        if (e != cudaSuccess) return cuda_fail(c, e, "packing the wide weight image");
+        GELL_CUDA(c, cudaStreamSynchronize(c->stream));
     }
     c->sur[sub] = S;
     if (fresh) {
@@ -1593,9 +1283,6 @@ gell_status gell_surrogate_load(gell_ctx* c, int sub, const float* weights, long
         gell_status st = plane_map(c, &S->map_in, S->in, 2);
         if (st == GELL_OK) st = plane_map(c, &S->map_h, S->h, 4);
         if (st == GELL_OK) st = plane_map(c, &S->map_t, S->t, 4);
-        if (st == GELL_OK) st = plane_map(c, &S->map_in_w, S->in, 2, kWN);
-        if (st == GELL_OK) st = plane_map(c, &S->map_h_w, S->h, 4, kWN);
-        if (st == GELL_OK) st = plane_map(c, &S->map_t_w, S->t, 4, kWN);
         if (st != GELL_OK) return st;
     }
     return GELL_OK;
@@ -1674,8 +1361,7 @@ gell_status gell_surrogate_train_init(gell_ctx* c, int sub, const float* weights
         for (int k = 0; ok && k < 5; ++k) ok = cudaMalloc(&T->hb[k], 4 * plane) == cudaSuccess;
         for (int k = 0; ok && k < 4; ++k) ok = cudaMalloc(&T->tb[k], 4 * plane) == cudaSuccess;
         for (int l = 1; ok && l < kLayers; ++l)
-            ok = cudaMalloc(&T->wt[l], (size_t)27 * (dgrad_cin8(l) / 2) * 2 * dgrad_nout(l) * 8 * 2) == cudaSuccess &&
-                 cudaMalloc(&T->wwt[l], (size_t)9 * (dgrad_cin8(l) / 2) * 128 * 32) == cudaSuccess;
+            ok = cudaMalloc(&T->wt[l], (size_t)27 * (dgrad_cin8(l) / 2) * 2 * dgrad_nout(l) * 8 * 2) == cudaSuccess;
         if (!ok) return fail(c, GELL_ERR_ALLOC, "surrogate training buffers (46 planes of 16 bytes per voxel)");
         GELL_CUDA(c, cudaMemsetAsync(T->zero_bias, 0, 32 * 4, c->stream));
         GELL_CUDA(c, cudaMemsetAsync(T->gd, 0, 2 * plane, c->stream));
@@ -1686,11 +1372,6 @@ gell_status gell_surrogate_train_init(gell_ctx* c, int sub, const float* weights
         if (st == GELL_OK) st = plane_map(c, &T->mgu, T->gu, 4);
         if (st == GELL_OK) st = plane_map(c, &T->mgh_g, T->gh, 4, kTileM);
         if (st == GELL_OK) st = plane_map(c, &T->mgu_g, T->gu, 4, kTileM);
-        for (int k = 0; k < 5 && st == GELL_OK; ++k) st = plane_map(c, &T->mh_w[k], T->hb[k], 4, kWN);
-        for (int k = 0; k < 4 && st == GELL_OK; ++k) st = plane_map(c, &T->mt_w[k], T->tb[k], 4, kWN);
-        if (st == GELL_OK) st = plane_map(c, &T->mgd_w, T->gd, 2, kWN);
-        if (st == GELL_OK) st = plane_map(c, &T->mgh_w, T->gh, 4, kWN);
-        if (st == GELL_OK) st = plane_map(c, &T->mgu_w, T->gu, 4, kWN);
         if (st != GELL_OK) return st;
     }
     TrainState* T = S->train;

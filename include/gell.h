@@ -273,11 +273,7 @@ gell_status gell_sort_keys_noalloc(const int32_t* keys, int32_t* sorted_keys, in
 /* Options (none has a reference counterpart).  GELL_OPT_EXACT_CHAIN = 1 makes the LOD back
  * substitution run the exact division chain for every group instead of the speculative chain that
  * is checked against it; results are identical either way, this only makes the exact path testable. */
-enum { GELL_OPT_EXACT_CHAIN = 1, GELL_OPT_SWEEP_WARPS = 3, GELL_OPT_CONV_RING = 4, GELL_OPT_CONV_WIDE = 5 };
-/* GELL_OPT_CONV_WIDE (0 or 1): the surrogate's convolutions put the weights in the MMA's A operand
- * (rows = x tap and output channel) and 144 staged voxels in B, so each MMA is 4.5x wider and a
- * tile takes 18 MMAs instead of 54; the epilogue sums the three x taps.  Same results up to the
- * order of fp32 sums. */
+enum { GELL_OPT_EXACT_CHAIN = 1, GELL_OPT_SWEEP_WARPS = 3, GELL_OPT_CONV_RING = 4 };
 /* GELL_OPT_CONV_RING (0 or 1, default 1): the surrogate's convolutions keep the input rows of
  * consecutive lines in a ring of shared-memory slots (each row read from L2 once per unit of 32
  * lines) instead of loading all nine rows per tile; the results are the same. */

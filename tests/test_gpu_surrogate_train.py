@@ -87,12 +87,10 @@ def layer_slices():
     return out
 
 
-@pytest.mark.parametrize("wide", [1, 0])
 @pytest.mark.parametrize("N", [40, 136])
-def test_training_gradient_matches_autograd(N, wide):
+def test_training_gradient_matches_autograd(N):
     w = random_weights(21)
     with make_sim(N, 9) as sim:
-        sim.set_conv_wide(bool(wide))
         sim.surrogate_train_init(0, w, 5, 0.1)
         p = sim.field(0)
         loss = sim.surrogate_train_pair(0, 0.0)
