@@ -3,8 +3,9 @@ judge's calibration.
 
 The operator, its training step and its judge run in the library (gell_surrogate_train_pair,
 gell_lod_surrogate: hand-written tcgen05 kernels); this module drives the fit and the
-calibration.  Training pairs come from the plain LOD solver (the reference's LODsolver, include/LODkernel.cuh:280-300, bit-exact in this library):
-input (p, uptake map, shell) -> p after `substeps` substeps, over seeded jittered-lattice
+calibration.  Training pairs come from the plain LOD solver (the reference's LODsolver,
+include/LODkernel.cuh:280-300, bit-exact in this library): input (p, uptake map, shell) -> p
+after `substeps` substeps, over seeded jittered-lattice
 spheroids with the large plain-method workload's statistics (volume fraction 0.6, radii N(5, 0.5)
 um) placed at random centres with seeded Ki-67 states.  The surrogate stands in for the substeps of
 a quasi-steady field between mechanics steps, so each spheroid's field is first relaxed from the
