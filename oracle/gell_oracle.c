@@ -402,6 +402,52 @@ void go_move(go_cell* cells, int n, const go_params* P) {
     }
 }
 
+/* FP64 restatement of forcekernel and movementkernel (include/FMkernel.cuh:56-118,130-158), for the
+ * accuracy report rather than parity: the same bins, candidate order and stale cutoff as
+ * go_force_one, every operation in double.  `cells` are sorted with `s`/`e` their cell list; writes
+ * the force and the moved position (pos + dt/2 (3 f - oldforce)) of every live cell, zeros for
+ * the others. */
+void go_force_move_f64(const go_cell* cells, int n, const go_params* P, const int* s, const int* e, double* force,
+                       double* pos) {
+    const int N = P->N;
+    const double h = (double)P->mech_dt / 2.0;
+#pragma omp parallel for OMP_THREADS schedule(dynamic, 256)
+    for (int i = 0; i < n; ++i) {
+        double* f = force + 3L * i;
+        double* q = pos + 3L * i;
+        f[0] = f[1] = f[2] = q[0] = q[1] = q[2] = 0.0;
+        if (!cells[i].sign) continue;
+        const double x1 = cells[i].pos[0], y1 = cells[i].pos[1], z1 = cells[i].pos[2], r1 = cells[i].r;
+        int b[3];
+        go_find_mesh(cells[i].pos, P->len, b);
+        double fx = 0.0, fy = 0.0, fz = 0.0, thres = P->cc_max_dist;
+        for (int xi = b[0] - 1; xi <= b[0] + 1; ++xi)
+            for (int yi = b[1] - 1; yi <= b[1] + 1; ++yi)
+                for (int zi = b[2] - 1; zi <= b[2] + 1; ++zi) {
+                    if (!go_inside(xi, yi, zi, N)) continue;
+                    long m = vidx(xi, yi, zi, N);
+                    if (e[m] < 0) continue;
+                    for (int j = s[m]; j <= e[m]; ++j) {
+                        if (!cells[j].sign) continue;
+                        const double dx = x1 - cells[j].pos[0], dy = y1 - cells[j].pos[1], dz = z1 - cells[j].pos[2];
+                        const double d = sqrt(dx * dx + dy * dy + dz * dz + 0.0001);
+                        if (d >= thres) continue;
+                        const double rs = cells[j].r + r1, R = rs > 0.01 ? rs : 0.01;
+                        thres = R * P->ra_ratio;
+                        if (d >= thres) continue;
+                        double coefr = 0.0, coefa = 0.0;
+                        if (d <= R) coefr = P->cccr * ((1.0 - d / R) * (1.0 - d / R) / d);
+                        if (d <= thres) coefa = P->ccca * ((1.0 - d / thres) * (1.0 - d / thres) / d);
+                        fx += dx * (coefr - coefa);
+                        fy += dy * (coefr - coefa);
+                        fz += dz * (coefr - coefa);
+                    }
+                }
+        f[0] = fx; f[1] = fy; f[2] = fz;
+        for (int a = 0; a < 3; ++a) q[a] = cells[i].pos[a] + h * (3.0 * f[a] - cells[i].oldforce[a]);
+    }
+}
+
 void go_fm_update(go_cell* cells, int n, const go_params* P, int* keys, int* perm, int* s, int* e) {
     long NNN = (long)P->N * P->N * P->N;
     int* k = keys ? keys : (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));

@@ -82,6 +82,9 @@ void go_force_one(const go_cell* cells, int i, const go_params* P, const int* s,
                   float out[3]);
 /* movementkernel (:130-158) */
 void go_move(go_cell* cells, int n, const go_params* P);
+/* FP64 force and moved position of each live sorted cell (accuracy report, not parity) */
+void go_force_move_f64(const go_cell* cells, int n, const go_params* P, const int* s, const int* e, double* force,
+                       double* pos);
 /* FM_update (:181-202): keys, sort, s/e, force, move.  keys/perm/s/e may be NULL. */
 void go_fm_update(go_cell* cells, int n, const go_params* P, int* keys, int* perm, int* s, int* e);
 

@@ -65,6 +65,10 @@ def lib() -> ctypes.CDLL:
         L.go_stable_sort.argtypes = [P, P, I, P]
         L.go_cell_list.argtypes = [P, I, P, P, P]
         L.go_force.argtypes = [P, I, P, P, P]
+        L.go_update_keys.argtypes = [P, I, P, P]
+        L.go_stable_sort.argtypes = [P, P, I, P]
+        L.go_cell_list.argtypes = [P, I, P, P, P]
+        L.go_force_move_f64.argtypes = [P, I, P, P, P, P, P]
         L.go_force_one.argtypes = [P, I, P, P, P, P]
         L.go_move.argtypes = [P, I, P]
         L.go_fm_update.argtypes = [P, I, P, P, P, P, P]
@@ -151,6 +155,25 @@ def fm_update(cells, P: GoParams):
     e = np.zeros(NNN, np.int32)
     lib().go_fm_update(ptr(cells), n, ctypes.byref(P), ptr(keys), ptr(perm), ptr(s), ptr(e))
     return keys[:n], perm[:n], s, e
+
+
+def force_move_f64(cells, P: GoParams):
+    """The cells sorted as FM_update sorts them, and the FP64 force and moved position of each
+    live one: (sorted cells, force[n,3], pos[n,3])."""
+    c = np.ascontiguousarray(cells).copy()
+    n = len(c)
+    NNN = P.N ** 3
+    keys = np.zeros(max(n, 1), np.int32)
+    perm = np.zeros(max(n, 1), np.int32)
+    s = np.zeros(NNN, np.int32)
+    e = np.zeros(NNN, np.int32)
+    lib().go_update_keys(ptr(c), n, ctypes.byref(P), ptr(keys))
+    lib().go_stable_sort(ptr(c), ptr(keys), n, ptr(perm))
+    lib().go_cell_list(ptr(c), n, ctypes.byref(P), ptr(s), ptr(e))
+    f = np.zeros((max(n, 1), 3), np.float64)
+    q = np.zeros((max(n, 1), 3), np.float64)
+    lib().go_force_move_f64(ptr(c), n, ctypes.byref(P), ptr(s), ptr(e), ptr(f), ptr(q))
+    return c, f[:n], q[:n]
 
 
 def force_one(cells, i, P, s, e):

@@ -123,3 +123,19 @@ def test_birth_philox_appends_in_mother_order():
     # each daughter and its mother sit symmetric about the mother's old position
     centre = (d["pos"].astype(np.float64) + m["pos"]) / 2
     np.testing.assert_allclose(centre, c["pos"], atol=1e-3)
+
+
+def test_fm_fp32_close_to_fp64():
+    """The FP32 restatement of forcekernel + movementkernel against its FP64 restatement: forces
+    within 1e-5 of the largest force, positions within 1e-4 um."""
+    from cases import ball_cells
+    cells = ball_cells(32, 10.0, 3000, seed=7)
+    P = ol.params(N=32, len=10.0, cap=6000)
+    srt, f64, p64 = ol.force_move_f64(cells, P)
+    c32 = cells.copy()
+    ol.fm_update(c32, P)
+    alive = (srt["sign"] != 0) & (c32["sign"] != 0)
+    assert alive.sum() > 2500
+    fs = np.abs(f64[alive]).max()
+    assert np.abs(c32["oldforce"][alive] - f64[alive]).max() < 1e-5 * fs
+    assert np.abs(c32["pos"][alive] - p64[alive]).max() < 1e-4
