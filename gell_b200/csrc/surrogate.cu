@@ -935,7 +935,6 @@ struct SurrogateState {
     unsigned* dmax = nullptr;   // judge scratch
     unsigned* hmax = nullptr;   // pinned host copy
     CUtensorMap map_in, map_h, map_t;
-    double conv_flops = 0;      // algorithmic FLOPs of one inference (real channels only)
     struct TrainState* train = nullptr;
 };
 
@@ -1249,7 +1248,6 @@ gell_status gell_surrogate_load(gell_ctx* c, int sub, const float* weights, long
     S->substeps = substeps;
     S->rate_scale = rate_scale;
     S->threshold = threshold;
-    S->conv_flops = 0;
     const float* W = weights;
     for (int l = 0; l < kLayers; ++l) {
         const LayerShape& s = kShape[l];
@@ -1259,7 +1257,6 @@ gell_status gell_surrogate_load(gell_ctx* c, int sub, const float* weights, long
         std::vector<float> bias(s.nout, 0.f);
         for (int n = 0; n < s.cout; ++n) bias[n] = W[n];
         W += s.cout;
-        S->conv_flops += 2.0 * (double)c->nvox * s.cout * s.cin * 27;
         if (!S->w[l]) {
             c->sur[sub] = S;  // owned by the context from here on (freed with it)
             if (cudaMalloc(&S->w[l], img.size() * 2) != cudaSuccess || cudaMalloc(&S->bias[l], bias.size() * 4) != cudaSuccess)
