@@ -69,7 +69,7 @@ def make_sim(N, seed, cells=2000):
 
 
 @pytest.mark.parametrize("ring", [1, 0])
-@pytest.mark.parametrize("N", [40, 136])
+@pytest.mark.parametrize("N", [40, 136, 37])
 def test_surrogate_layers_match_torch(N, ring):
     w = random_weights(3)
     Ws = layer_params(w)

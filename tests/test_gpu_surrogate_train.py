@@ -87,7 +87,7 @@ def layer_slices():
     return out
 
 
-@pytest.mark.parametrize("N", [40, 136])
+@pytest.mark.parametrize("N", [40, 136, 37])
 def test_training_gradient_matches_autograd(N):
     w = random_weights(21)
     with make_sim(N, 9) as sim:
