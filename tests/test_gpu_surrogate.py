@@ -185,3 +185,39 @@ def test_packaged_surrogate_vs_fp64_oracle():
         assert e_sur <= 0.01
     else:
         assert np.array_equal(q.view(np.uint32), plain.view(np.uint32))
+
+
+def test_surrogate_step_touches_only_its_substrate():
+    """A judged oxygen step in a context that also holds the drug: the drug field is left as it was,
+    and a rejected step gives oxygen exactly the plain solver's substeps of oxygen alone."""
+    N, K = 40, 50
+    w = random_weights(8)
+    with make_sim(N, 11) as a, make_sim(N, 11) as ref:
+        for sim in (a, ref):
+            sim.add_substrate(gb.drug())
+            sim.set_field(1, random_field(N, 12, 0.2, 1.0))
+            sim.PreLOD()
+        drug0 = a.field(1)
+        a.surrogate_load(0, w, K, 0.1, -1.0)  # every step rejected
+        ok, _ = a.lod_surrogate(0)
+        assert not ok
+        ref.LODsolver(K, 0)
+        assert np.array_equal(a.field(0).view(np.uint32), ref.field(0).view(np.uint32))
+        assert np.array_equal(a.field(1).view(np.uint32), drug0.view(np.uint32))
+        a.sync()
+
+
+def test_surrogate_errors_are_reported():
+    import ctypes
+    L = gb.load_library()
+    with make_sim(24, 13) as sim:
+        w = random_weights(9)
+        # wrong weight count, no surrogate loaded, bad substrate: errors, and the context goes on
+        assert L.gell_surrogate_load(sim.h, 0, w.ctypes.data, w.size - 1, 50, 0.1, 1e-3) == -1
+        acc, r = ctypes.c_int(), ctypes.c_float()
+        assert L.gell_lod_surrogate(sim.h, 0, ctypes.byref(acc), ctypes.byref(r)) == -1
+        assert L.gell_surrogate_load(sim.h, 3, w.ctypes.data, w.size, 50, 0.1, 1e-3) == -1
+        sim.surrogate_load(0, w, 50, 0.1, 1e9)
+        ok, _ = sim.lod_surrogate(0)
+        assert ok
+        sim.sync()
