@@ -15,9 +15,10 @@ both substrates.
              copies are the ABI's queued transfers, which overlap the LOD substeps
   roofline   the kernel with the largest device time in the timed region, against HBM
 
-`--impl reference` times the CPU restatement of the reference's hot path (the oracle, OpenMP on
-the host cores) on the same workload, each step a bounded sample: one FM_update and PreLOD on
-all cells and one LOD substep, extrapolated to the step's ten substeps of both substrates.
+`--impl reference` times the reference's own CUDA build on the same GPU: its kernels and facades
+compiled from its unmodified sources (oracle/_ref), whole steps of the same workload, with the
+same e2e contract.  `cpu_baseline` times the reference's kernel bodies compiled for the host with
+OpenMP (oracle/_ref/libgellref_host_*), two whole steps on the host cores.
 
 Multi-GPU: every rank runs its own replica (the path has no exchange step); value = cells of all
 ranks / max time over ranks.
@@ -636,82 +637,208 @@ def run_c4(args, rank, world, local_rank):
     return line
 
 
-# ---------------------------------------------------------------------------- CPU (oracle) leg
+# ---------------------------------------------------------------------------- CPU baseline
 
-class CpuWork:
-    """The oracle (C, OpenMP) on the same workload: FM_update + PreLOD on all cells and one LOD
-    substep of one substrate per sample; substep time extrapolated to 10 substeps x 2 substrates."""
+CPU_STEPS = 2
 
-    def __init__(self):
+
+def cpu_baseline():
+    """The reference's own FM and LOD kernel bodies compiled for the host with OpenMP
+    (oracle/_ref/libgellref_host_c2{,d}.so, see oracle/ref_host_harness.cpp), on this machine's
+    host cores: CPU_STEPS whole steps of the same workload (FM_update, PreLOD of both substrates,
+    10 LODsolver substeps of both), after one untimed FM_update and substep that touch every array.
+    Where the host build is missing, the oracle's restatement runs the same steps (kind "port")."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import reference_build as rb
+
+    cells = make_cells()
+    if rb.host_available("c2") and rb.host_available("c2d"):
+        o2 = rb.HostRefSim("c2", 38.0, 1e5, 0.1)
+        dr = rb.HostRefSim("c2d", 1.0, 5e4, 0.05)
+        o2.set_cells(cells)
+        o2.fm_update()
+        o2.prelod()
+        dr.prelod_on(o2)
+        o2.lodsolver(1)
+        dr.lodsolver(1)
+        o2.set_cells(cells)
+        t = [0.0, 0.0, 0.0]
+        for _ in range(CPU_STEPS):
+            t0 = time.perf_counter()
+            o2.fm_update()
+            t1 = time.perf_counter()
+            o2.prelod()
+            dr.prelod_on(o2)
+            t2 = time.perf_counter()
+            o2.lodsolver(SUBSTEPS)
+            dr.lodsolver(SUBSTEPS)
+            t3 = time.perf_counter()
+            t[0] += t1 - t0
+            t[1] += t2 - t1
+            t[2] += t3 - t2
+        alive = int(o2.cells()["sign"].sum())
+        cores = o2.threads
+        o2.close()
+        dr.close()
+        kind = "reference"
+        what = ("the reference's FM and LOD kernel bodies compiled for the host (g++ -O3 -fopenmp, "
+                "oracle/_ref/libgellref_host_c2{,d}.so)")
+    else:
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         import oracle_lib as ol
-        self.ol = ol
-        self.P = ol.params(N=N, len=LENGTH, cap=CAP)
-        self.cells = make_cells()
-        self.subs = [(38.0, 1e5, 0.1, -10.0), (1.0, 5e4, 0.05, -1.0)]
-        self.EF = [ol.mesh_init(N, LENGTH, D, dec, 0.01) for (_, D, dec, _) in self.subs]
-        self.field = [np.full(N ** 3, b, np.float32) for (b, _, _, _) in self.subs]
-        self.k = 0
-
-    def cores(self):
-        return self.ol.lib().go_get_threads()
-
-    def sample(self):
-        ol = self.ol
-        t0 = time.perf_counter()
-        ol.fm_update(self.cells, self.P)
-        t1 = time.perf_counter()
-        rates = [ol.prelod(self.cells, N, LENGTH, coef) for (_, _, _, coef) in self.subs]
-        t2 = time.perf_counter()
-        s = self.k % NSUB
-        E, F = self.EF[s]
-        L = ol.lib()
-        L.go_lod_substep(self.field[s].ctypes.data, rates[s].ctypes.data, E.ctypes.data, F.ctypes.data,
-                         N, 0.01, self.subs[s][0])
-        t3 = time.perf_counter()
-        self.k += 1
-        alive = int(self.cells["sign"].sum())
-        return alive, t1 - t0, t2 - t1, t3 - t2
-
-    def rates(self, samples):
-        fm = np.mean([s[1] for s in samples])
-        pre = np.mean([s[2] for s in samples])
-        lod = np.mean([s[3] for s in samples])
-        alive = samples[-1][0]
-        step = fm + pre + SUBSTEPS * NSUB * lod
-        return {"value": alive / step, "step_s": step, "fm_s": fm, "prelod_s": pre, "lod_substep_s": lod,
-                "mech_rate": alive / (fm + pre), "vox_rate": N ** 3 / lod}
+        P = ol.params(N=N, len=LENGTH, cap=CAP)
+        subs = [(38.0, 1e5, 0.1, -10.0), (1.0, 5e4, 0.05, -1.0)]
+        EF = [ol.mesh_init(N, LENGTH, D, dec, 0.01) for (_, D, dec, _) in subs]
+        fields = [np.full(N ** 3, b, np.float32) for (b, _, _, _) in subs]
+        c = cells.copy()
+        t = [0.0, 0.0, 0.0]
+        for _ in range(CPU_STEPS):
+            t0 = time.perf_counter()
+            ol.fm_update(c, P)
+            t1 = time.perf_counter()
+            rates = [ol.prelod(c, N, LENGTH, coef) for (_, _, _, coef) in subs]
+            t2 = time.perf_counter()
+            for k in range(NSUB):
+                fields[k] = ol.lod_substeps(fields[k], rates[k], EF[k][0], EF[k][1], N, 0.01, subs[k][0], SUBSTEPS)
+            t3 = time.perf_counter()
+            t[0] += t1 - t0
+            t[1] += t2 - t1
+            t[2] += t3 - t2
+        alive = int(c["sign"].sum())
+        cores = int(ol.lib().go_get_threads())
+        kind = "port"
+        what = "the oracle's C restatement of the reference (OpenMP)"
+    step = sum(t) / CPU_STEPS
+    return {"value": alive / step, "unit": "cell-updates/s", "cores": cores, "kind": kind,
+            "sample": f"{CPU_STEPS} whole steps of the large workload on {what}: {step:.2f} s per step",
+            "s_per_step": step, "cell_updates_per_s_fm_prelod": alive * CPU_STEPS / (t[0] + t[1]),
+            "voxel_updates_per_s_lod": N ** 3 * NSUB * SUBSTEPS * CPU_STEPS / t[2]}
 
 
-def cpu_baseline(n_samples=3):
-    w = CpuWork()
-    samples = [w.sample() for _ in range(n_samples)]
-    r = w.rates(samples)
-    return {"value": r["value"], "unit": "cell-updates/s", "cores": w.cores(), "kind": "port",
-            "sample": (f"{n_samples} samples of FM_update + PreLOD on all 10^6 cells and one 400^3 LOD "
-                       f"substep; step time = FM + PreLOD + 20 x substep ({r['step_s']:.2f} s)"),
-            "voxel_updates_per_s": r["vox_rate"], "cell_updates_per_s_fm_prelod": r["mech_rate"]}
+def reference_unavailable(why):
+    return {"impl": "reference", "unavailable": why}
 
 
-def run_reference(args):
-    w = CpuWork()
+def run_reference(args, local_rank, world):
+    """The reference's own CUDA build on this GPU: its kernels and facades compiled from its
+    unmodified sources (oracle/_ref/libgellref_c2.so for oxygen, libgellref_c2d.so for the drug,
+    nvcc -O3 for sm_100a), driven as its host loop drives them (Main.cu:108-128) with integer
+    counts.  One step = FM_update (include/FMkernel.cuh:181-202), PreLOD of both substrates
+    (include/LODkernel.cuh:270-278) and 10 LODsolver substeps of both (:280-300); every facade
+    synchronises the device, as the reference does.  Whole steps are timed with CUDA events on the
+    legacy default stream the facades launch on.  e2e repeats the steps with the 72-byte cell
+    records copied in from pinned host memory before each step and back out after it.  Under
+    torchrun only rank 0 runs it, on one GPU (the line says n_gpus 1)."""
+    if world > 1:
+        # the reference selects no device: use this rank's before any CUDA call
+        os.environ["CUDA_VISIBLE_DEVICES"] = str(local_rank)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import reference_build as rb
+
+    missing = [n for n in ("c2", "c2d") if not rb.available(n)]
+    if missing:
+        return reference_unavailable(f"reference build oracle/_ref/libgellref_{missing[0]}.so is missing "
+                                     "(make -C oracle ref needs the reference sources)")
+    cells = make_cells()
+    o2 = rb.RefSim("c2", 38.0, 1e5, 0.1)
+    drug = rb.RefSim("c2d", 1.0, 5e4, 0.05)
+    o2.set_cells(cells)
+    ncell = len(cells)
+
+    def step():
+        o2.fm_update()
+        o2.prelod()
+        drug.prelod_on(o2)
+        o2.lodsolver(SUBSTEPS)
+        drug.lodsolver(SUBSTEPS)
+
     for _ in range(args.warmup):
-        w.sample()
-    samples = [w.sample() for _ in range(args.steps)]
-    r = w.rates(samples)
-    base = {"value": r["value"], "unit": "cell-updates/s", "cores": w.cores(), "kind": "port",
-            "sample": ("each step: FM_update + PreLOD on all 10^6 cells and one 400^3 LOD substep of one "
-                       "substrate (alternating); step time = FM + PreLOD + 20 x substep")}
+        step()
+    assert rb.lib("c2").gref_sync() == 0
+    sampler = ClockSampler(gpu_uuid_from_smi(local_rank))
+    sampler.start()
+    time.sleep(0.3)
+    ev = [rb.RefEvent("c2") for _ in range(2)]
+    K = args.steps
+    ev[0].record()
+    for _ in range(K):
+        step()
+    ev[1].record()
+    t_all = ev[0].elapsed_ms(ev[1])
+    sampler.stop()
+    alive = int(o2.cells()["sign"].sum())
+
+    # breakdown by facade, a separate pass with events between the facades
+    kc = max(1, min(K, 5))
+    pe = [rb.RefEvent("c2") for _ in range(4)]
+    t_fm = t_pre = t_lod = 0.0
+    for _ in range(kc):
+        pe[0].record()
+        o2.fm_update()
+        pe[1].record()
+        o2.prelod()
+        drug.prelod_on(o2)
+        pe[2].record()
+        o2.lodsolver(SUBSTEPS)
+        drug.lodsolver(SUBSTEPS)
+        pe[3].record()
+        t_fm += pe[0].elapsed_ms(pe[1])
+        t_pre += pe[1].elapsed_ms(pe[2])
+        t_lod += pe[2].elapsed_ms(pe[3])
+    t_fm, t_pre, t_lod = t_fm * K / kc, t_pre * K / kc, t_lod * K / kc
+
+    # e2e: the cell records in from pinned host memory and back out, every step
+    host = rb.PinnedCells("c2", ncell)
+    host.cells[:] = o2.cells()
+    ke = max(1, min(K, 20))
+    ev[0].record()
+    for _ in range(ke):
+        o2.set_cells(host.cells)
+        step()
+        o2.get_cells_into(host.cells)
+    ev[1].record()
+    t_e2e = ev[0].elapsed_ms(ev[1])
+    alive_e2e = int(host.cells["sign"].sum())
+    host.close()
+    for e in ev + pe:
+        e.close()
+    drug.close()
+    o2.close()
+
+    cnt = (alive * K, alive_e2e * ke)
+    t_mech = t_fm + t_pre
     return {
-        "impl": "reference", "metric": METRIC, "value": r["value"], "unit": "cell-updates/s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["step_s"] * 1e3,
+        "impl": "reference", "metric": METRIC, "value": cnt[0] / (t_all / 1e3), "unit": "cell-updates/s",
+        "n_gpus": 1, "ranks_launched": world, "steps": K, "warmup": args.warmup, "ms_per_step": t_all / K,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: seeded jittered-lattice spheroid of 10^6 cells, fields start at the boundary values",
-        "config": config({"parallelism": "host cores (rank 0 only)"}),
-        "components": {"cell_updates_per_s_fm_prelod": r["mech_rate"], "voxel_updates_per_s_lod": r["vox_rate"]},
-        "cpu_baseline": base,
-        "e2e": {"value": r["value"], "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "config": config(),
+        "reference_build": {
+            "what": "the reference's own kernels and facades, compiled from its unmodified sources",
+            "libraries": ["oracle/_ref/libgellref_c2.so", "oracle/_ref/libgellref_c2d.so"],
+            "compile": "nvcc -O3 -gencode arch=compute_100a,code=sm_100a (oracle/Makefile, oracle/ref_harness.cu)",
+            "step": "FM_update, PreLOD x 2 substrates, 10 x LODsolver x 2 substrates; integer loop counts"},
+        "components": {"cell_updates_per_s_fm_prelod": cnt[0] / (t_mech / 1e3),
+                       "voxel_updates_per_s_lod": N ** 3 * NSUB * SUBSTEPS * K / (t_lod / 1e3),
+                       "ms_fm_update": t_fm / K, "ms_prelod": t_pre / K, "ms_lod_10_substeps": t_lod / K},
+        "e2e": {"value": cnt[1] / (t_e2e / 1e3), "unit": "cell-updates/s", "steps": ke,
+                "h2d_bytes_per_step": int(ncell * 72), "d2h_bytes_per_step": int(ncell * 72)},
+        "clocks": sampler.summary(),
     }
+
+
+def gpu_uuid_from_smi(index):
+    """UUID of GPU `index` as nvidia-smi prints it (None when unavailable)."""
+    try:
+        out = subprocess.run(["nvidia-smi", "--query-gpu=index,uuid", "--format=csv,noheader"],
+                             capture_output=True, text=True, timeout=20).stdout
+        for line in out.splitlines():
+            i, u = [x.strip() for x in line.split(",", 1)]
+            if int(i) == int(index):
+                return u
+    except Exception:
+        pass
+    return None
 
 
 # ---------------------------------------------------------------------------- main
@@ -737,8 +864,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
 
     if args.impl == "reference":
+        # rank 0 alone runs the reference build (on its GPU); the other ranks exit without work
         if rank == 0:
-            print(json.dumps(run_reference(args)), flush=True)
+            print(json.dumps(run_reference(args, local_rank, world)), flush=True)
         return
 
     if world > 1:

@@ -198,6 +198,35 @@ int gref_set_field(void* h, const float* in) {
     size_t nb = sizeof(float) * (size_t)Voxel_num * Voxel_num * Voxel_num;
     return ok(cudaMemcpy(g->mesh->p, in, nb, cudaMemcpyHostToDevice));
 }
+// Mesh_struct::PreLOD on cells held by another handle (a second substrate is a second build of the
+// reference: its mesh takes the cells the first build's FM_update moved), and their device address
+void* gref_cells_ptr(void* h) { return thrust::raw_pointer_cast(((GRef*)h)->cells->data()); }
+int gref_prelod_ptr(void* h, void* dev_cells, int n) {
+    GRef* g = (GRef*)h;
+    g->mesh->PreLOD(static_cast<Cell*>(dev_cells), n);
+    return ok(cudaDeviceSynchronize());
+}
+
+// CUDA events on the legacy default stream, where every reference façade runs
+void* gref_event_create() {
+    cudaEvent_t e = nullptr;
+    return cudaEventCreate(&e) == cudaSuccess ? (void*)e : nullptr;
+}
+int gref_event_record(void* e) { return ok(cudaEventRecord((cudaEvent_t)e, 0)); }
+float gref_event_elapsed_ms(void* a, void* b) {
+    if (cudaEventSynchronize((cudaEvent_t)b) != cudaSuccess) return -1.f;
+    float ms = -1.f;
+    return cudaEventElapsedTime(&ms, (cudaEvent_t)a, (cudaEvent_t)b) == cudaSuccess ? ms : -1.f;
+}
+void gref_event_destroy(void* e) { cudaEventDestroy((cudaEvent_t)e); }
+int gref_sync() { return ok(cudaDeviceSynchronize()); }
+// page-locked host memory for the cells copied in and out around each step
+void* gref_host_alloc(size_t bytes) {
+    void* p = nullptr;
+    return cudaMallocHost(&p, bytes) == cudaSuccess ? p : nullptr;
+}
+void gref_host_free(void* p) { cudaFreeHost(p); }
+
 int gref_get_rate(void* h, float* out) {
     GRef* g = (GRef*)h;
     size_t nb = sizeof(float) * (size_t)Voxel_num * Voxel_num * Voxel_num;
