@@ -166,6 +166,74 @@ def test_birth_counts_chi_squared_over_seeds():
         assert abs(obs.mean() - mean) < 5 * np.sqrt(var / len(obs))
 
 
+def ki67_probabilities(o2):
+    """Per-biology-step probabilities of Cell::Phase_update_ki67adv (include/Cells.cuh:145-165) at
+    oxygen level o2, computed as the reference does (float ramps times double rates, stored as
+    float): proliferation, apoptosis, necrosis."""
+    f = np.float32
+    pro = float(f(f(f(1.0) * (f(o2) - f(5.0))) / (f(10.0) - f(5.0))) * (1.0 / 8.5 / 60.0) * 6.0)
+    if o2 > 10.0:
+        pro = float(f((1.0 / 8.5 / 60.0) * 6.0))
+    elif o2 < 5.0:
+        pro = 0.0
+    apo = float(f((1.0 / 7.0 / 24.0 / 60.0) * 6.0))
+    nec = float(f(f(f(1.0) * (f(5.0) - f(o2))) / (f(5.0) - f(2.5))) * (1.0 / 6.0 / 60.0) * 6.0)
+    if o2 > 5.0:
+        nec = 0.0
+    elif o2 < 2.5:
+        nec = float(f((1.0 / 6.0 / 60.0) * 6.0))
+    return pro, apo, nec
+
+
+@pytest.mark.parametrize("o2", [2.0, 4.0, 7.0, 12.0])
+def test_phase_transitions_chi_squared_on_the_oxygen_ramps(o2):
+    """Quiescent cells at a uniform oxygen level inside the proliferation ramp (7), above it (12),
+    inside the necrosis ramp (4) and below it (2): counts of the three stochastic transitions over
+    1000 Philox draws (successive biology steps) against their binomial laws.  A second population of
+    dead cells, half of them shrinking below the removal threshold in this step, checks the removal
+    count of CellDeath_kernel against the oracle on every draw."""
+    N, length = 32, 10.0
+    n = 4000
+    base = ball_cells(N, length, n, seed=31, outside=0, dead_frac=0.0)
+    base["phase"] = 0
+    base["cell_clock"] = 0.0
+    nd = 400
+    dead = ball_cells(N, length, nd, seed=32, outside=0, dead_frac=0.0)
+    dead["phase"] = 3
+    dead["Vcs"] = np.where(np.arange(nd) % 2 == 0, np.float32(24.0), np.float32(400.0))
+    cells = np.concatenate([base, dead])
+    # oracle: which dead cells are removed (deterministic: Volume_update, then Vcs <= 24.4)
+    oc = np.concatenate([cells, gb.empty_cells(2 * len(cells))])
+    field = np.full(N ** 3, o2, np.float32)
+    ol.birth_philox(oc, len(cells), ol.params(N=N, len=length, cap=len(oc)), field, 5, 0)
+    removed_exp = int((oc["sign"][n:len(cells)] == 0).sum())
+    assert 0 < removed_exp < nd
+    p = ki67_probabilities(o2)
+    counts = {1: [], 3: [], 4: []}
+    with gb.Simulation(voxel_num=N, voxel_length=length, max_cell_num=65536,
+                       rng_mode=gb.GELL_RNG_PHILOX, seed=9000 + int(o2 * 10)) as sim:
+        sim.add_substrate(gb.oxygen())
+        sim.set_field(0, field)
+        for _ in range(1000):
+            sim.import_cells(cells)
+            nb = sim.CellBirth_kernel()
+            out = sim.export_cells()
+            for ph in counts:
+                counts[ph].append(int((out["phase"][:n] == ph).sum()))
+            assert nb == len(cells)  # quiescent cells do not divide within the step
+            assert sim.CellDeath_kernel() == len(cells) - removed_exp
+    for ph, prob in zip((1, 3, 4), p):
+        obs = np.array(counts[ph])
+        if prob == 0.0:
+            assert obs.sum() == 0, ph
+            continue
+        mean, var = n * prob, n * prob * (1 - prob)
+        chi2 = float(np.sum((obs - mean) ** 2 / var))
+        # 1000 degrees of freedom: mean 1000, sd ~45-50; reject beyond ~5 sd
+        assert 760 < chi2 < 1250, (ph, chi2, obs.mean(), mean)
+        assert abs(obs.mean() - mean) < 5 * np.sqrt(var / len(obs)), (ph, obs.mean(), mean)
+
+
 @pytest.mark.skipif(not ref_lib.available("t32"), reason="reference build oracle/_ref missing")
 def test_volume_update_contraction_vs_reference_device():
     """Cell::Volume_update as the reference's device build computes it (include/Cells.cuh:91-143),
