@@ -384,6 +384,15 @@ class Simulation:
         """Run every LOD back-substitution group on the exact division chain (same results)."""
         self._check(self.lib.gell_set_option(self.h, 1, int(bool(on))), "gell_set_option")
 
+    def set_sweep_warps(self, warps: int) -> None:
+        """Line tiles per CTA of the LOD sweeps (0 = as many as fit; the ring sweeps use twice as many
+        warps); results do not change."""
+        self._check(self.lib.gell_set_option(self.h, 3, int(warps)), "gell_set_option")
+
+    def set_sweep_ring(self, on: bool = True) -> None:
+        """LOD sweeps as ring kernels (more warps per SM, same results) or whole line tiles."""
+        self._check(self.lib.gell_set_option(self.h, 5, int(bool(on))), "gell_set_option")
+
     def set_conv_ring(self, on: bool = True) -> None:
         """The surrogate's convolutions with (default) or without the row ring along y."""
         self._check(self.lib.gell_set_option(self.h, 4, int(bool(on))), "gell_set_option")

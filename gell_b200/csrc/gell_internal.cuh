@@ -118,7 +118,9 @@ struct gell_ctx {
     bool rate_valid = false;
     bool exact_chain = false;  // GELL_OPT_EXACT_CHAIN
     int sweep_warps = 0;       // GELL_OPT_SWEEP_WARPS (0: as many as shared memory allows)
+    bool sweep_ring = false;   // GELL_OPT_SWEEP_RING: ring sweeps instead of whole line tiles
     bool sweeps_configured = false;  // the sweeps' shared-memory attribute is set on this device
+    bool ring_configured = false;    // the same for the ring sweeps
 
     // gell_run_mechanics: captured graphs of two mechanics steps and what each was captured for
     // (two entries: an odd number of steps flips the double buffers to the other assignment)

@@ -197,7 +197,7 @@ __device__ __forceinline__ void reset8(float v[8], int j0, const XReset& r) {
 
 // Forward elimination over group g: Y_j = fma(-E_j, Y_{j-1}, p_j) for the 32 elements of the group,
 // 8 at a time with the next batch's values and E already requested.
-template <int AXIS>
+template <int AXIS, bool STORE = true>
 __device__ __forceinline__ void forward_group(const SweepCtx& c, float* slot, int g, int lane, float& Y, bool rs,
                                               const XReset& xr) {
     const int j0 = 32 * g;
@@ -220,7 +220,7 @@ __device__ __forceinline__ void forward_group(const SweepCtx& c, float* slot, in
             Y = __fmaf_rn(-ev[k], Y, v[k]);
             v[k] = Y;
         }
-        store8<AXIS>(slot, 8 * b8, lane, v);
+        if (STORE) store8<AXIS>(slot, 8 * b8, lane, v);
         if (b8 < 3) {
 #pragma unroll
             for (int k = 0; k < 8; ++k) v[k] = w[k];
@@ -294,7 +294,7 @@ __device__ __forceinline__ void backward_full(const SweepCtx& c, float* slot, in
 // The same two steps for a group whose E and F are the line's converged constants (all lanes'
 // lines share them): the factors live in registers, and independent multiply-adds are issued in
 // pairs (FFMA2), without changing any operation or its rounding.
-template <int AXIS>
+template <int AXIS, bool STORE = true>
 __device__ __forceinline__ void forward_uniform(float* slot, int g, int lane, float& Y, float nE, bool rs,
                                                 const XReset& xr) {
     float v[8], w[8];
@@ -308,7 +308,7 @@ __device__ __forceinline__ void forward_uniform(float* slot, int g, int lane, fl
             Y = __fmaf_rn(nE, Y, v[k]);
             v[k] = Y;
         }
-        store8<AXIS>(slot, 8 * b8, lane, v);
+        if (STORE) store8<AXIS>(slot, 8 * b8, lane, v);
         if (b8 < 3) {
 #pragma unroll
             for (int k = 0; k < 8; ++k) v[k] = w[k];
@@ -539,6 +539,200 @@ __global__ void __launch_bounds__(64 * kMaxComputeWarps, 1) k_sweep(const __grid
     }
 }
 
+// ------------------------------------------------------------------ ring sweeps
+//
+// The kernel above keeps a whole 32-line tile in shared memory from its forward elimination to its
+// back substitution, so shared memory bounds the lines in flight (4 compute warps per SM at
+// N = 400, 2 at N = 600) and the dependent recurrences of those few warps leave the SM idle most
+// of the time.  This variant needs only R group slots of 4 KB per warp, R < B, so 8 compute warps
+// fit at both sizes:
+//   * forward elimination streams the B groups of the tile through the ring; for the groups
+//     [0, B-R) it keeps only the running value Y entering the group (a checkpoint, 4 B per lane
+//     and group in shared memory) and frees the slot at once;
+//   * the top R groups stay resident with their Y values, as in the kernel above;
+//   * back substitution takes the groups from the top down; a group below B-R is loaded again
+//     (the second read of the tile hits L2: the tile was read a few tens of microseconds before)
+//     and its Y values are recomputed from the checkpoint with the same operations, so they are
+//     bit-identical to the first pass; results go back to the field by TMA stores.
+// Each compute warp issues its own copies (lane 0), always into a slot whose previous occupant it
+// has finished with: loads run R (forward) or R-1 (back) groups ahead of their use.  Group g of a
+// tile of parity q lives in slot  g mod R  (q = 0) or  R-1 - (g mod R)  (q = 1), which makes the
+// slots the back substitution frees last the ones the next tile's first groups take.
+constexpr int kRingWarps = 8;
+constexpr int kRingMaxSlots = 8;
+
+__device__ __forceinline__ int ring_slot(int g, int q, int R) {
+    const int m = g % R;
+    return q ? R - 1 - m : m;
+}
+
+// Bounded clean-up after a failed wait: wait (briefly) for every load still in flight into this
+// warp's slots and for its stores, so no copy outlives the CTA's shared memory.
+__device__ __forceinline__ void ring_drain(uint64_t* full, uint32_t pend, uint32_t phase, int R, int* err, int lane) {
+    for (int s = 0; s < R; ++s)
+        if ((pend >> s) & 1u) mbar_wait(full + s, (phase >> s) & 1u, err, 20, 1 << 16);
+    if (lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    __syncwarp();
+}
+
+template <int AXIS>
+__device__ __forceinline__ bool ring_tile(const LodArgs& a, const TileDesc& d, const TileDesc& dn, bool has_next,
+                                          int q, int R, float* buf, uint64_t* full, float* ck, const float* sE,
+                                          int Na, uint32_t& phase, uint32_t& pend) {
+    const int N = a.g.N;
+    const int B = (N + 31) >> 5;
+    const int keep = B - R;  // groups [keep, B) stay resident between the two passes
+    const int lane = threadIdx.x & 31;
+    const SubDev& sd = a.sub[d.s];
+    SweepCtx c;
+    c.E = sE + (size_t)d.s * Na;
+    c.FR = sd.FRS;
+    c.b = sd.b;
+    c.dt = a.dt;
+    uint32_t special = 0;
+    XReset xr{0, 0, c.b};
+    if (AXIS == 0) {
+        const bool sp = !d.flagged_lane && !d.interior_lane;
+        xr.lo = d.flagged_lane ? 1 : (d.interior_lane ? 2 : 0x7fffffff);
+        xr.hi = d.flagged_lane ? N - 2 : N - 3;
+        special = __ballot_sync(FULL, sp);
+    }
+    auto wait_slot = [&](int s) -> bool {
+        if (!mbar_wait(full + s, (phase >> s) & 1u, a.err, 1 + AXIS)) return false;
+        phase ^= 1u << s;
+        pend &= ~(1u << s);
+        return true;
+    };
+    auto load = [&](const TileDesc& t, int g, int s) {
+        if (lane == 0) box_load<AXIS>(a, t, g, buf + (size_t)s * kSlotFloats, full + s);
+        pend |= 1u << s;
+    };
+    // one group's forward elimination from the running value Y, storing Y into the slot or not
+    auto forward = [&](float* slot, int g, float& Y, bool store) {
+        const bool edge = g == 0 || 32 * g + 31 > N - 3;
+        const bool rs = AXIS == 0 && (edge || special != 0);
+        if (AXIS != 0 && edge) edge_rows<AXIS>(c, slot, g, N, lane);
+        const bool uni = (sd.uni >> g) & 1u;
+        if (store) {
+            if (uni) forward_uniform<AXIS, true>(slot, g, lane, Y, sd.nE, rs, xr);
+            else forward_group<AXIS, true>(c, slot, g, lane, Y, rs, xr);
+        } else {
+            if (uni) forward_uniform<AXIS, false>(slot, g, lane, Y, sd.nE, rs, xr);
+            else forward_group<AXIS, false>(c, slot, g, lane, Y, rs, xr);
+        }
+    };
+
+    float Y = c.b;
+    for (int g = 0; g < B; ++g) {
+        const int s = ring_slot(g, q, R);
+        if (!wait_slot(s)) return false;
+        float* slot = buf + (size_t)s * kSlotFloats;
+        if (g < keep) {
+            ck[g * 32 + lane] = Y;
+            forward(slot, g, Y, false);
+            fence_proxy_async();  // the edge rows may have written the slot
+            __syncwarp();
+            load(d, g + R, s);  // same slot: (g + R) mod R == g mod R
+        } else {
+            forward(slot, g, Y, true);
+        }
+    }
+    float x = c.b;
+    for (int h = B - 1; h >= 0; --h) {
+        const int s = ring_slot(h, q, R);
+        float* slot = buf + (size_t)s * kSlotFloats;
+        if (h < keep) {
+            if (!wait_slot(s)) return false;
+            float Yh = ck[h * 32 + lane];
+            forward(slot, h, Yh, true);  // the same Y values as the first pass
+        }
+        backward_group<AXIS>(c, sd, slot, h, lane, x, a.exact);
+        // results in the slot: visible to the TMA store, then stored
+        fence_proxy_async();
+        __syncwarp();
+        if (lane == 0) {
+            box_store<AXIS>(a, d, h, slot);
+            bulk_commit();
+        }
+        if (h < B - 1) {
+            // the slot of group h+1: its store (one group ago) has read it by now
+            const int s1 = ring_slot(h + 1, q, R);
+            if (h + 1 >= R) {
+                if (lane == 0) bulk_wait_read<1>();
+                load(d, h + 1 - R, s1);  // back substitution's second read of group h+1-R
+            } else if (has_next) {
+                if (lane == 0) bulk_wait_read<1>();
+                load(dn, R - 2 - h, s1);  // next tile (parity 1-q), group R-2-h
+            }
+        }
+        if (h == 0 && has_next) {
+            if (lane == 0) bulk_wait_read<0>();
+            load(dn, R - 1, s);  // next tile, group R-1, into this group's slot
+        }
+        __syncwarp();
+    }
+    return true;
+}
+
+template <int AXIS>
+__global__ void __launch_bounds__(32 * kRingWarps, 1) k_sweep_ring(const __grid_constant__ LodArgs a, int R) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    const Geom g = a.g;
+    const int N = g.N, P = g.P;
+    const int Na = (N + 31) & ~31;
+    const int B = (N + 31) >> 5;
+    const int W = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t base = smem_u32(sm);
+    unsigned char* sm1 = sm + ((1024 - (base & 1023)) & 1023);
+    float* slots = reinterpret_cast<float*>(sm1);
+    size_t off = (size_t)W * R * kSlotFloats * 4;
+    float* sE = reinterpret_cast<float*>(sm1 + off);
+    off += align128(a.nsub * Na * 4);
+    float* cks = reinterpret_cast<float*>(sm1 + off);
+    off += align128(W * B * 32 * 4);
+    uint64_t* full = reinterpret_cast<uint64_t*>(sm1 + off);
+    for (int i = threadIdx.x; i < a.nsub * Na; i += blockDim.x) {
+        const int s = i / Na, j = i - s * Na;
+        sE[i] = (j >= 1 && j <= N - 2) ? a.sub[s].EFR[j] : 0.f;
+    }
+    for (int i = threadIdx.x; i < W * R; i += blockDim.x) mbar_init(full + i, 1u);
+    fence_mbar_init();
+    __syncthreads();
+
+    long long per_sub;
+    if (AXIS == 0) per_sub = ((long long)N * N + 31) / 32;
+    else if (AXIS == 1) per_sub = (long long)((P + 31) / 32) * N;
+    else per_sub = (g.PN + 31) / 32;
+    const long long total = per_sub * a.nsub;
+    const long long step = (long long)gridDim.x * W;
+
+    long long t = (long long)blockIdx.x * W + warp;
+    if (t >= total) return;
+    float* buf = slots + (size_t)warp * R * kSlotFloats;
+    uint64_t* fb = full + warp * R;
+    float* ck = cks + (size_t)warp * B * 32;
+    uint32_t phase = 0, pend = 0;
+    TileDesc d = tile_desc<AXIS>(a, t, per_sub);
+    // the first tile's first R groups
+    for (int gg = 0; gg < R; ++gg) {
+        if (lane == 0) box_load<AXIS>(a, d, gg, buf + (size_t)ring_slot(gg, 0, R) * kSlotFloats, fb + ring_slot(gg, 0, R));
+        pend |= 1u << ring_slot(gg, 0, R);
+    }
+    for (int k = 0;; ++k) {
+        const long long tn = t + step;
+        const bool has_next = tn < total;
+        const TileDesc dn = has_next ? tile_desc<AXIS>(a, tn, per_sub) : d;
+        if (!ring_tile<AXIS>(a, d, dn, has_next, k & 1, R, buf, fb, ck, sE, Na, phase, pend)) {
+            ring_drain(fb, pend, phase, R, a.err, lane);
+            return;
+        }
+        if (!has_next) break;
+        t = tn;
+        d = dn;
+    }
+    if (lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
 // The bounded wait's give-up path: nothing ever arrives on this barrier, so the wait must stop after
 // `polls` polls and record code 12 in the context's error word, as a sweep does when a box never
 // lands.  Run by gell_selftest_timeout; the context stays usable afterwards.
@@ -703,6 +897,69 @@ gell_status prelod(gell_ctx* c, int sub) {
     return GELL_OK;
 }
 
+// The ring sweeps (k_sweep_ring): W warps per CTA, each with R group slots, R as large as shared
+// memory allows (at most kRingMaxSlots, at least 2 unless a line is one group).
+static gell_status lod_solver_ring(gell_ctx* c, const LodArgs& ax, const LodArgs& ay, const LodArgs& az, int s0,
+                                   int s1, int substeps) {
+    const int ns = ax.nsub;
+    const int N = c->g.N;
+    const int B = (N + 31) / 32;
+    const int Na = (N + 31) & ~31;
+    const int smem_cap = 227 * 1024;
+    int W = c->sweep_warps > 0 ? 2 * c->sweep_warps : kRingWarps;
+    if (W > kRingWarps) W = kRingWarps;
+    int R = 0;
+    for (; W >= 1; W /= 2) {
+        const int fixed = 1024 + align128(ns * Na * 4) + align128(W * B * 32 * 4) + W * kRingMaxSlots * 8;
+        R = (smem_cap - fixed) / (W * kSlotFloats * 4);
+        if (R > kRingMaxSlots) R = kRingMaxSlots;
+        if (R > B) R = B;
+        if (R >= 2 || (B == 1 && R == 1)) break;
+    }
+    if (W < 1) return fail(c, GELL_ERR_UNSUPPORTED, "grid edge too large for the ring sweeps");
+    const int smem = 1024 + W * R * kSlotFloats * 4 + align128(ns * Na * 4) + align128(W * B * 32 * 4) + W * R * 8;
+    if (!c->ring_configured) {
+        GELL_CUDA(c, cudaFuncSetAttribute(k_sweep_ring<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
+        GELL_CUDA(c, cudaFuncSetAttribute(k_sweep_ring<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
+        GELL_CUDA(c, cudaFuncSetAttribute(k_sweep_ring<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
+        c->ring_configured = true;
+    }
+    const long long xt = ((long long)N * N + 31) / 32 * ns;
+    const long long yt = (long long)((c->g.P + 31) / 32) * N * ns;
+    const long long zt = (c->g.PN + 31) / 32 * ns;
+    auto grid = [&](long long tiles, const void* kern) {
+        int occ = 1;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, W * 32, smem) != cudaSuccess || occ < 1) {
+            cudaGetLastError();
+            occ = 1;
+        }
+        long long want = (tiles + W - 1) / W;
+        long long cap = (long long)num_sms() * occ;
+        return (int)(want < cap ? want : cap);
+    };
+    const int gx = grid(xt, (const void*)k_sweep_ring<0>), gy = grid(yt, (const void*)k_sweep_ring<1>),
+              gz = grid(zt, (const void*)k_sweep_ring<2>);
+    SrcArgs sa{};
+    for (int s = s0; s < s1; ++s) {
+        const Substrate& S = c->subs[s];
+        sa.p[sa.nsub] = S.p;
+        sa.rate[sa.nsub] = S.rate;
+        sa.list[sa.nsub] = S.line_list;
+        sa.count[sa.nsub] = S.line_count;
+        sa.b[sa.nsub] = S.s.boundary;
+        sa.nsub++;
+    }
+    sa.g = c->g;
+    sa.dt = c->P.diffusion_dt;
+    for (int k = 0; k < substeps; ++k) {
+        GELL_KERNEL(c, "k_source_lines", k_source_lines<<<num_sms() * 8, 256, 0, c->stream>>>(sa));
+        GELL_KERNEL(c, "k_sweep_x", k_sweep_ring<0><<<gx, W * 32, smem, c->stream>>>(ax, R));
+        GELL_KERNEL(c, "k_sweep_y", k_sweep_ring<1><<<gy, W * 32, smem, c->stream>>>(ay, R));
+        GELL_KERNEL(c, "k_sweep_z", k_sweep_ring<2><<<gz, W * 32, smem, c->stream>>>(az, R));
+    }
+    return GELL_OK;
+}
+
 gell_status lod_solver(gell_ctx* c, int sub, int substeps) {
     if (c->subs.empty() || substeps == 0) return GELL_OK;
     LodArgs ax{}, ay{}, az{};
@@ -731,6 +988,7 @@ gell_status lod_solver(gell_ctx* c, int sub, int substeps) {
     const int B = (N + 31) / 32;
     const int Na = (N + 31) & ~31;
     const int smem_cap = 227 * 1024;
+    if (c->sweep_ring) return lod_solver_ring(c, ax, ay, az, s0, s1, substeps);
     const int fixed = 1024 + align128(ns * Na * 4) + 2 * 8 * 32 * 8;
     int w = (smem_cap - fixed) / (B * kSlotFloats * 4);
     w = w > kMaxComputeWarps ? kMaxComputeWarps : w;

@@ -262,18 +262,27 @@ gell_status gell_selftest_timeout(gell_ctx* ctx, int polls);
  * that must keep to a memory budget reserved up front, C callers that only own their buffers.  So
  * this call allocates nothing: keys, sorted_keys and perm are the caller's device buffers, and the
  * scratch lives in one fixed device array inside the library (about 8.3 MB on every GPU that
- * loads it, kept until the process exits).  key_bits = bits of the largest key + 1 (e.g. 28 on a
- * 400^3 grid).  n above GELL_NOALLOC_MAX_KEYS returns GELL_ERR_CAPACITY.  The first call on a
- * device looks up that device's scratch address and should come before any stream capture; all
- * calls share the scratch, so calls that overlap on the GPU race.  Work is queued on `stream`
- * (a cudaStream_t; NULL = the default stream) and not synchronised. */
+ * loads it, kept until the process exits).  key_bits must be at least the bit length of
+ * (largest key + 1), e.g. 27 on a 400^3 grid; a smaller value gives an unspecified order, with
+ * status OK.  keys, sorted_keys and perm must not share any memory (GELL_ERR_INVALID_ARG
+ * otherwise).  n above GELL_NOALLOC_MAX_KEYS returns GELL_ERR_CAPACITY.  A CUDA error already
+ * pending on the calling thread when the call starts is returned as GELL_ERR_CUDA and left
+ * pending.  The first call on a device (and under each further driver context of it) looks up the
+ * scratch address and should come before any stream capture; after a cudaDeviceReset the entry
+ * point must not be called again.  All calls share the scratch, so calls that overlap on the GPU
+ * race.  Work is queued on `stream` (a cudaStream_t; NULL = the default stream) and not
+ * synchronised. */
 gell_status gell_sort_keys_noalloc(const int32_t* keys, int32_t* sorted_keys, int32_t* perm, int n,
                                    int key_bits, void* stream);
 
 /* Options (none has a reference counterpart).  GELL_OPT_EXACT_CHAIN = 1 makes the LOD back
  * substitution run the exact division chain for every group instead of the speculative chain that
  * is checked against it; results are identical either way, this only makes the exact path testable. */
-enum { GELL_OPT_EXACT_CHAIN = 1, GELL_OPT_SWEEP_WARPS = 3, GELL_OPT_CONV_RING = 4 };
+enum { GELL_OPT_EXACT_CHAIN = 1, GELL_OPT_SWEEP_WARPS = 3, GELL_OPT_CONV_RING = 4, GELL_OPT_SWEEP_RING = 5 };
+/* GELL_OPT_SWEEP_RING (0 or 1): 1 runs the LOD sweeps as ring kernels (a few group slots of shared
+ * memory per warp, back substitution re-reads each group from L2 and recomputes its forward values
+ * from a per-group checkpoint), which fit twice as many warps per SM; 0 keeps whole line tiles in
+ * shared memory.  Results are identical either way. */
 /* GELL_OPT_CONV_RING (0 or 1, default 1): the surrogate's convolutions keep the input rows of
  * consecutive lines in a ring of shared-memory slots (each row read from L2 once per unit of 32
  * lines) instead of loading all nine rows per tile; the results are the same. */
