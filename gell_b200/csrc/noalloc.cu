@@ -12,10 +12,15 @@
 // The array is a static __device__ object: every GPU that loads the library holds it (about
 // 8.3 MB) until the process exits.  In host code its name is only a host-side stand-in, so the
 // device address is looked up once per device with cudaGetSymbolAddress, with that device
-// current, on the first call made on that device; that first call should therefore come before
-// any stream capture.  All calls share the one array and it keeps the last call's contents:
-// nothing in it needs to start at zero (every table entry is written before it is read), and two
-// calls whose work overlaps on the GPU race on it.
+// current, on the first call made on that device (and again on the first call under another
+// driver context of the device); that first call should therefore come before any stream
+// capture.  A cudaDeviceReset can leave a cached address stale (a new primary context may reuse
+// the old handle), so a process that resets a device must not call this entry point again.  All
+// calls share the one array and it keeps the last call's contents: nothing in it needs to start
+// at zero (every table entry is written before it is read), and two calls whose work overlaps on
+// the GPU race on it.  The call neither allocates nor frees anything.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "gell_internal.cuh"
@@ -143,24 +148,64 @@ __global__ void __launch_bounds__(kNaThreads) na_scatter(const uint32_t* __restr
     }
 }
 
-// Device address of the scratch array, looked up once per device (with that device current).
+// Device address of the scratch array, looked up with the device current and cached per device
+// together with the driver context it was looked up in: a call made under another context of the
+// same device (a non-primary context, or a primary context created anew) looks the address up again.
+struct NaScratch {
+    void* ctx;
+    uint32_t* ptr;
+};
 std::mutex g_na_mutex;
-uint32_t* g_na_ptr[64] = {nullptr};
+NaScratch g_na_cache[64] = {};
+
+using CtxGetCurrent = CUresult (*)(CUcontext*);
+
+cudaError_t current_context(void** out) {
+    static CtxGetCurrent fn = nullptr;
+    if (!fn) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q);
+        if (e != cudaSuccess) return e;
+        if (q != cudaDriverEntryPointSuccess || !f) return cudaErrorNotSupported;
+        fn = reinterpret_cast<CtxGetCurrent>(f);
+    }
+    CUcontext c = nullptr;
+    if (fn(&c) != CUDA_SUCCESS) return cudaErrorDeviceUninitialized;
+    *out = c;
+    return cudaSuccess;
+}
 
 cudaError_t scratch_for_current_device(uint32_t** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    void* ctx = nullptr;  // null before the runtime has made the device's primary context current
+    e = current_context(&ctx);
+    if (e != cudaSuccess) return e;
     std::lock_guard<std::mutex> lock(g_na_mutex);
-    if (!g_na_ptr[dev]) {
+    NaScratch& c = g_na_cache[dev];
+    if (!c.ptr || !ctx || c.ctx != ctx) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return e;
-        g_na_ptr[dev] = static_cast<uint32_t*>(p);
+        if (!ctx) {
+            e = current_context(&ctx);
+            if (e != cudaSuccess) return e;
+        }
+        c.ptr = static_cast<uint32_t*>(p);
+        c.ctx = ctx;
     }
-    *out = g_na_ptr[dev];
+    *out = c.ptr;
     return cudaSuccess;
+}
+
+// Whether [a, a + n) and [b, b + n) (int32 elements) share any byte.
+bool overlap(const void* a, const void* b, int n) {
+    const uintptr_t x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
+    const uintptr_t len = (uintptr_t)n * sizeof(int32_t);
+    return x < y + len && y < x + len;
 }
 
 }  // namespace
@@ -174,10 +219,16 @@ extern "C" gell_status gell_sort_keys_noalloc(const int32_t* keys, int32_t* sort
     if (key_bits < 1 || key_bits > 32) return GELL_ERR_INVALID_ARG;
     if (n > GELL_NOALLOC_MAX_KEYS) return GELL_ERR_CAPACITY;
     if (n == 0) return GELL_OK;
+    // pass 0 reads keys while (for an odd pass count) it writes the outputs, and the passes use
+    // sorted_keys and perm as two separate ping-pong buffers: the three must not share memory
+    if (overlap(keys, sorted_keys, n) || overlap(keys, perm, n) || overlap(sorted_keys, perm, n))
+        return GELL_ERR_INVALID_ARG;
+    // an error left pending by the caller's earlier work is reported as it is, not consumed here
+    if (cudaPeekAtLastError() != cudaSuccess) return GELL_ERR_CUDA;
     uint32_t* scratch = nullptr;
     cudaError_t e = scratch_for_current_device(&scratch);
     if (e != cudaSuccess) {
-        cudaGetLastError();
+        cudaGetLastError();  // the failed look-up's own error
         return e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver ? GELL_ERR_NO_DEVICE : GELL_ERR_CUDA;
     }
     cudaStream_t s = (cudaStream_t)stream;
