@@ -389,9 +389,14 @@ class Simulation:
         warps); results do not change."""
         self._check(self.lib.gell_set_option(self.h, 3, int(warps)), "gell_set_option")
 
-    def set_sweep_ring(self, on: bool = True) -> None:
-        """LOD sweeps as ring kernels (more warps per SM, same results) or whole line tiles."""
-        self._check(self.lib.gell_set_option(self.h, 5, int(bool(on))), "gell_set_option")
+    def set_sweep_ring(self, on=True) -> None:
+        """LOD sweeps as ring kernels (more warps per SM, same results): True/1, or 2..8 = at most
+        that many group slots per warp; False/0 = whole line tiles; -1 = automatic (the default)."""
+        self._check(self.lib.gell_set_option(self.h, 5, int(on)), "gell_set_option")
+
+    def set_sweep_l2hint(self, on: bool = True) -> None:
+        """The ring sweeps' L2 eviction priorities (same results)."""
+        self._check(self.lib.gell_set_option(self.h, 6, int(bool(on))), "gell_set_option")
 
     def set_conv_ring(self, on: bool = True) -> None:
         """The surrogate's convolutions with (default) or without the row ring along y."""

@@ -678,7 +678,11 @@ gell_status gell_set_option(gell_ctx* c, int option, int64_t value) {
             c->sweep_warps = (int)value;
             return GELL_OK;
         case GELL_OPT_CONV_RING: c->conv_ring = value != 0; return GELL_OK;
-        case GELL_OPT_SWEEP_RING: c->sweep_ring = value != 0; return GELL_OK;
+        case GELL_OPT_SWEEP_RING:
+            if (value < -1 || value > 8) return fail(c, GELL_ERR_INVALID_ARG, "sweep ring outside -1..8");
+            c->sweep_ring = (int)value;
+            return GELL_OK;
+        case GELL_OPT_SWEEP_L2HINT: c->sweep_l2hint = value != 0; return GELL_OK;
         default: return fail(c, GELL_ERR_INVALID_ARG, "unknown option");
     }
 }

@@ -118,7 +118,8 @@ struct gell_ctx {
     bool rate_valid = false;
     bool exact_chain = false;  // GELL_OPT_EXACT_CHAIN
     int sweep_warps = 0;       // GELL_OPT_SWEEP_WARPS (0: as many as shared memory allows)
-    bool sweep_ring = false;   // GELL_OPT_SWEEP_RING: ring sweeps instead of whole line tiles
+    int sweep_ring = -1;       // GELL_OPT_SWEEP_RING: -1 auto, 0 line tiles, 1 ring, >= 2 ring of at most that many slots
+    bool sweep_l2hint = false;  // GELL_OPT_SWEEP_L2HINT: the ring sweeps' L2 eviction priorities
     bool sweeps_configured = false;  // the sweeps' shared-memory attribute is set on this device
     bool ring_configured = false;    // the same for the ring sweeps
 

@@ -129,6 +129,15 @@ __device__ __forceinline__ void box_load(const LodArgs& a, const TileDesc& d, in
     else if (AXIS == 1) tma_load_3d(slot, &a.tm[d.s], d.c0, 32 * g, d.c2, bar);
     else tma_load_2d(slot, &a.tm[d.s], d.c0, 32 * g, bar);
 }
+// The same load with an L2 eviction-priority policy.
+template <int AXIS>
+__device__ __forceinline__ void box_load_hint(const LodArgs& a, const TileDesc& d, int g, float* slot, uint64_t* bar,
+                                              uint64_t pol) {
+    mbar_arrive_expect(bar, kSlotFloats * 4);
+    if (AXIS == 0) tma_load_2d_hint(slot, &a.tm[d.s], 32 * g, d.c0, bar, pol);
+    else if (AXIS == 1) tma_load_3d_hint(slot, &a.tm[d.s], d.c0, 32 * g, d.c2, bar, pol);
+    else tma_load_2d_hint(slot, &a.tm[d.s], d.c0, 32 * g, bar, pol);
+}
 template <int AXIS>
 __device__ __forceinline__ void box_store(const LodArgs& a, const TileDesc& d, int g, const float* slot) {
     if (AXIS == 0) tma_store_2d(&a.tm[d.s], 32 * g, d.c0, slot);
@@ -575,7 +584,7 @@ __device__ __forceinline__ void ring_drain(uint64_t* full, uint32_t pend, uint32
     __syncwarp();
 }
 
-template <int AXIS>
+template <int AXIS, bool HINT>
 __device__ __forceinline__ bool ring_tile(const LodArgs& a, const TileDesc& d, const TileDesc& dn, bool has_next,
                                           int q, int R, float* buf, uint64_t* full, float* ck, const float* sE,
                                           int Na, uint32_t& phase, uint32_t& pend) {
@@ -603,8 +612,14 @@ __device__ __forceinline__ bool ring_tile(const LodArgs& a, const TileDesc& d, c
         pend &= ~(1u << s);
         return true;
     };
-    auto load = [&](const TileDesc& t, int g, int s) {
-        if (lane == 0) box_load<AXIS>(a, t, g, buf + (size_t)s * kSlotFloats, full + s);
+    // with HINT, a group that will be read a second time is loaded with priority to stay in L2 and
+    // every other load (a last read) with priority to leave it first
+    auto load = [&](const TileDesc& t, int g, int s, bool again) {
+        if (lane == 0) {
+            if (HINT) box_load_hint<AXIS>(a, t, g, buf + (size_t)s * kSlotFloats, full + s,
+                                          again ? l2_evict_last() : l2_evict_first());
+            else box_load<AXIS>(a, t, g, buf + (size_t)s * kSlotFloats, full + s);
+        }
         pend |= 1u << s;
     };
     // one group's forward elimination from the running value Y, storing Y into the slot or not
@@ -632,7 +647,7 @@ __device__ __forceinline__ bool ring_tile(const LodArgs& a, const TileDesc& d, c
             forward(slot, g, Y, false);
             fence_proxy_async();  // the edge rows may have written the slot
             __syncwarp();
-            load(d, g + R, s);  // same slot: (g + R) mod R == g mod R
+            load(d, g + R, s, g + R < keep);  // same slot: (g + R) mod R == g mod R
         } else {
             forward(slot, g, Y, true);
         }
@@ -659,22 +674,22 @@ __device__ __forceinline__ bool ring_tile(const LodArgs& a, const TileDesc& d, c
             const int s1 = ring_slot(h + 1, q, R);
             if (h + 1 >= R) {
                 if (lane == 0) bulk_wait_read<1>();
-                load(d, h + 1 - R, s1);  // back substitution's second read of group h+1-R
+                load(d, h + 1 - R, s1, false);  // back substitution's second read of group h+1-R
             } else if (has_next) {
                 if (lane == 0) bulk_wait_read<1>();
-                load(dn, R - 2 - h, s1);  // next tile (parity 1-q), group R-2-h
+                load(dn, R - 2 - h, s1, R - 2 - h < keep);  // next tile (parity 1-q), group R-2-h
             }
         }
         if (h == 0 && has_next) {
             if (lane == 0) bulk_wait_read<0>();
-            load(dn, R - 1, s);  // next tile, group R-1, into this group's slot
+            load(dn, R - 1, s, R - 1 < keep);  // next tile, group R-1, into this group's slot
         }
         __syncwarp();
     }
     return true;
 }
 
-template <int AXIS>
+template <int AXIS, bool HINT>
 __global__ void __launch_bounds__(32 * kRingWarps, 1) k_sweep_ring(const __grid_constant__ LodArgs a, int R) {
     extern __shared__ __align__(1024) unsigned char sm[];
     const Geom g = a.g;
@@ -715,14 +730,19 @@ __global__ void __launch_bounds__(32 * kRingWarps, 1) k_sweep_ring(const __grid_
     TileDesc d = tile_desc<AXIS>(a, t, per_sub);
     // the first tile's first R groups
     for (int gg = 0; gg < R; ++gg) {
-        if (lane == 0) box_load<AXIS>(a, d, gg, buf + (size_t)ring_slot(gg, 0, R) * kSlotFloats, fb + ring_slot(gg, 0, R));
+        if (lane == 0) {
+            float* sl = buf + (size_t)ring_slot(gg, 0, R) * kSlotFloats;
+            if (HINT) box_load_hint<AXIS>(a, d, gg, sl, fb + ring_slot(gg, 0, R),
+                                          gg < B - R ? l2_evict_last() : l2_evict_first());
+            else box_load<AXIS>(a, d, gg, sl, fb + ring_slot(gg, 0, R));
+        }
         pend |= 1u << ring_slot(gg, 0, R);
     }
     for (int k = 0;; ++k) {
         const long long tn = t + step;
         const bool has_next = tn < total;
         const TileDesc dn = has_next ? tile_desc<AXIS>(a, tn, per_sub) : d;
-        if (!ring_tile<AXIS>(a, d, dn, has_next, k & 1, R, buf, fb, ck, sE, Na, phase, pend)) {
+        if (!ring_tile<AXIS, HINT>(a, d, dn, has_next, k & 1, R, buf, fb, ck, sE, Na, phase, pend)) {
             ring_drain(fb, pend, phase, R, a.err, lane);
             return;
         }
@@ -906,22 +926,28 @@ static gell_status lod_solver_ring(gell_ctx* c, const LodArgs& ax, const LodArgs
     const int B = (N + 31) / 32;
     const int Na = (N + 31) & ~31;
     const int smem_cap = 227 * 1024;
+    const int rmax = c->sweep_ring >= 2 ? c->sweep_ring : kRingMaxSlots;
     int W = c->sweep_warps > 0 ? 2 * c->sweep_warps : kRingWarps;
     if (W > kRingWarps) W = kRingWarps;
     int R = 0;
     for (; W >= 1; W /= 2) {
         const int fixed = 1024 + align128(ns * Na * 4) + align128(W * B * 32 * 4) + W * kRingMaxSlots * 8;
         R = (smem_cap - fixed) / (W * kSlotFloats * 4);
-        if (R > kRingMaxSlots) R = kRingMaxSlots;
+        if (R > rmax) R = rmax;
         if (R > B) R = B;
         if (R >= 2 || (B == 1 && R == 1)) break;
     }
     if (W < 1) return fail(c, GELL_ERR_UNSUPPORTED, "grid edge too large for the ring sweeps");
     const int smem = 1024 + W * R * kSlotFloats * 4 + align128(ns * Na * 4) + align128(W * B * 32 * 4) + W * R * 8;
+    const bool hint = c->sweep_l2hint;
+    const void* kx = hint ? (const void*)k_sweep_ring<0, true> : (const void*)k_sweep_ring<0, false>;
+    const void* ky = hint ? (const void*)k_sweep_ring<1, true> : (const void*)k_sweep_ring<1, false>;
+    const void* kz = hint ? (const void*)k_sweep_ring<2, true> : (const void*)k_sweep_ring<2, false>;
     if (!c->ring_configured) {
-        GELL_CUDA(c, cudaFuncSetAttribute(k_sweep_ring<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
-        GELL_CUDA(c, cudaFuncSetAttribute(k_sweep_ring<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
-        GELL_CUDA(c, cudaFuncSetAttribute(k_sweep_ring<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
+        for (const void* k : {(const void*)k_sweep_ring<0, true>, (const void*)k_sweep_ring<1, true>,
+                              (const void*)k_sweep_ring<2, true>, (const void*)k_sweep_ring<0, false>,
+                              (const void*)k_sweep_ring<1, false>, (const void*)k_sweep_ring<2, false>})
+            GELL_CUDA(c, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
         c->ring_configured = true;
     }
     const long long xt = ((long long)N * N + 31) / 32 * ns;
@@ -937,8 +963,7 @@ static gell_status lod_solver_ring(gell_ctx* c, const LodArgs& ax, const LodArgs
         long long cap = (long long)num_sms() * occ;
         return (int)(want < cap ? want : cap);
     };
-    const int gx = grid(xt, (const void*)k_sweep_ring<0>), gy = grid(yt, (const void*)k_sweep_ring<1>),
-              gz = grid(zt, (const void*)k_sweep_ring<2>);
+    const int gx = grid(xt, kx), gy = grid(yt, ky), gz = grid(zt, kz);
     SrcArgs sa{};
     for (int s = s0; s < s1; ++s) {
         const Substrate& S = c->subs[s];
@@ -953,11 +978,27 @@ static gell_status lod_solver_ring(gell_ctx* c, const LodArgs& ax, const LodArgs
     sa.dt = c->P.diffusion_dt;
     for (int k = 0; k < substeps; ++k) {
         GELL_KERNEL(c, "k_source_lines", k_source_lines<<<num_sms() * 8, 256, 0, c->stream>>>(sa));
-        GELL_KERNEL(c, "k_sweep_x", k_sweep_ring<0><<<gx, W * 32, smem, c->stream>>>(ax, R));
-        GELL_KERNEL(c, "k_sweep_y", k_sweep_ring<1><<<gy, W * 32, smem, c->stream>>>(ay, R));
-        GELL_KERNEL(c, "k_sweep_z", k_sweep_ring<2><<<gz, W * 32, smem, c->stream>>>(az, R));
+        if (hint) {
+            GELL_KERNEL(c, "k_sweep_x", k_sweep_ring<0, true><<<gx, W * 32, smem, c->stream>>>(ax, R));
+            GELL_KERNEL(c, "k_sweep_y", k_sweep_ring<1, true><<<gy, W * 32, smem, c->stream>>>(ay, R));
+            GELL_KERNEL(c, "k_sweep_z", k_sweep_ring<2, true><<<gz, W * 32, smem, c->stream>>>(az, R));
+        } else {
+            GELL_KERNEL(c, "k_sweep_x", k_sweep_ring<0, false><<<gx, W * 32, smem, c->stream>>>(ax, R));
+            GELL_KERNEL(c, "k_sweep_y", k_sweep_ring<1, false><<<gy, W * 32, smem, c->stream>>>(ay, R));
+            GELL_KERNEL(c, "k_sweep_z", k_sweep_ring<2, false><<<gz, W * 32, smem, c->stream>>>(az, R));
+        }
     }
     return GELL_OK;
+}
+
+// Whether the line-tile kernels keep fewer than four line tiles per SM at this grid edge (a tile is
+// the whole line in shared memory), in which case the ring sweeps are used by default.
+static bool ring_by_default(const gell_ctx* c, int ns) {
+    const int N = c->g.N;
+    const int B = (N + 31) / 32;
+    const int Na = (N + 31) & ~31;
+    const int fixed = 1024 + align128(ns * Na * 4) + 2 * 8 * 32 * 8;
+    return (227 * 1024 - fixed) / (B * kSlotFloats * 4) < 4;
 }
 
 gell_status lod_solver(gell_ctx* c, int sub, int substeps) {
@@ -988,7 +1029,8 @@ gell_status lod_solver(gell_ctx* c, int sub, int substeps) {
     const int B = (N + 31) / 32;
     const int Na = (N + 31) & ~31;
     const int smem_cap = 227 * 1024;
-    if (c->sweep_ring) return lod_solver_ring(c, ax, ay, az, s0, s1, substeps);
+    if (c->sweep_ring > 0 || (c->sweep_ring < 0 && ring_by_default(c, ns)))
+        return lod_solver_ring(c, ax, ay, az, s0, s1, substeps);
     const int fixed = 1024 + align128(ns * Na * 4) + 2 * 8 * 32 * 8;
     int w = (smem_cap - fixed) / (B * kSlotFloats * 4);
     w = w > kMaxComputeWarps ? kMaxComputeWarps : w;

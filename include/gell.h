@@ -278,11 +278,20 @@ gell_status gell_sort_keys_noalloc(const int32_t* keys, int32_t* sorted_keys, in
 /* Options (none has a reference counterpart).  GELL_OPT_EXACT_CHAIN = 1 makes the LOD back
  * substitution run the exact division chain for every group instead of the speculative chain that
  * is checked against it; results are identical either way, this only makes the exact path testable. */
-enum { GELL_OPT_EXACT_CHAIN = 1, GELL_OPT_SWEEP_WARPS = 3, GELL_OPT_CONV_RING = 4, GELL_OPT_SWEEP_RING = 5 };
-/* GELL_OPT_SWEEP_RING (0 or 1): 1 runs the LOD sweeps as ring kernels (a few group slots of shared
- * memory per warp, back substitution re-reads each group from L2 and recomputes its forward values
- * from a per-group checkpoint), which fit twice as many warps per SM; 0 keeps whole line tiles in
- * shared memory.  Results are identical either way. */
+enum {
+    GELL_OPT_EXACT_CHAIN = 1,
+    GELL_OPT_SWEEP_WARPS = 3,
+    GELL_OPT_CONV_RING = 4,
+    GELL_OPT_SWEEP_RING = 5,
+    GELL_OPT_SWEEP_L2HINT = 6
+};
+/* GELL_OPT_SWEEP_RING (-1..8, default -1): 1 runs the LOD sweeps as ring kernels (a few group
+ * slots of shared memory per warp; back substitution re-reads each group from L2 and recomputes its
+ * forward values from a per-group checkpoint), which fit twice as many warps per SM as whole line
+ * tiles; 2..8 do the same with at most that many slots per warp; 0 keeps whole line tiles in shared
+ * memory; -1 picks the ring when fewer than four line tiles fit per SM (long lines, N > 416).
+ * GELL_OPT_SWEEP_L2HINT (0 or 1, default 0): the ring sweeps load groups they will read again with
+ * priority to stay in L2.  Results are identical for every value of either option. */
 /* GELL_OPT_CONV_RING (0 or 1, default 1): the surrogate's convolutions keep the input rows of
  * consecutive lines in a ring of shared-memory slots (each row read from L2 once per unit of 32
  * lines) instead of loading all nine rows per tile; the results are the same. */
