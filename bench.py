@@ -637,6 +637,40 @@ def run_c4(args, rank, world, local_rank):
     return line
 
 
+# ---------------------------------------------------------------------------- other workloads
+
+def other_workloads(args, local_rank):
+    """Short runs of the other workloads, after the headline measurement (single GPU only), so that
+    their figures travel with the headline line: the birth/death workload for one biology period
+    (60 mechanics steps), the ensemble for 20 steps, the surrogate for 5 blocks.  Each is the same
+    code as its own --workload line, with fewer steps; a failure is reported in place of its
+    figures."""
+    import gc
+
+    out = {}
+    runs = (("c3_600cube_5M_cells_birth_death", run_c3, 60),
+            ("c4_ensemble_64", run_c4, 20),
+            ("c5_surrogate_256cube", run_c5, 5))
+    for name, fn, steps in runs:
+        a = argparse.Namespace(**vars(args))
+        a.steps, a.warmup = steps, 3
+        t0 = time.time()
+        try:
+            r = fn(a, 0, 1, local_rank)
+            keep = {k: r[k] for k in ("value", "unit", "ms_per_step", "steps", "components", "clocks")
+                    if k in r}
+            for k in ("plain", "speedup_vs_plain", "accuracy", "roofline"):
+                if k in r:
+                    keep[k] = r[k]
+            keep["workload"] = r["config"]["workload"]
+            out[name] = keep
+        except Exception as e:  # the headline line is printed regardless
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+        out[name]["wall_s"] = round(time.time() - t0, 1)
+        gc.collect()
+    return out
+
+
 # ---------------------------------------------------------------------------- CPU baseline
 
 CPU_STEPS = 2
@@ -807,6 +841,7 @@ def run_reference(args, local_rank, world):
 
     cnt = (alive * K, alive_e2e * ke)
     t_mech = t_fm + t_pre
+    c5 = reference_lod_256(rb) if rb.available("c5") else None
     return {
         "impl": "reference", "metric": METRIC, "value": cnt[0] / (t_all / 1e3), "unit": "cell-updates/s",
         "n_gpus": 1, "ranks_launched": world, "steps": K, "warmup": args.warmup, "ms_per_step": t_all / K,
@@ -820,11 +855,42 @@ def run_reference(args, local_rank, world):
             "step": "FM_update, PreLOD x 2 substrates, 10 x LODsolver x 2 substrates; integer loop counts"},
         "components": {"cell_updates_per_s_fm_prelod": cnt[0] / (t_mech / 1e3),
                        "voxel_updates_per_s_lod": N ** 3 * NSUB * SUBSTEPS * K / (t_lod / 1e3),
-                       "ms_fm_update": t_fm / K, "ms_prelod": t_pre / K, "ms_lod_10_substeps": t_lod / K},
+                       "ms_fm_update": t_fm / K, "ms_prelod": t_pre / K, "ms_lod_10_substeps": t_lod / K,
+                       "lod_256cube_surrogate_workload": c5},
         "e2e": {"value": cnt[1] / (t_e2e / 1e3), "unit": "cell-updates/s", "steps": ke,
                 "h2d_bytes_per_step": int(ncell * 72), "d2h_bytes_per_step": int(ncell * 72)},
         "clocks": sampler.summary(),
     }
+
+
+def reference_lod_256(rb, blocks=3):
+    """The reference's own LODsolver (oracle/_ref/libgellref_c5.so: 256^3 voxels of 10 um, oxygen)
+    on the surrogate workload's state: the same 300,000-cell spheroid and Ki-67 states as
+    `--workload c5`, the field relaxed by the same 1000 substeps; then per block FM_update, PreLOD
+    and the 50 timed substeps the surrogate replaces.  Returns ms per block of 50 substeps."""
+    import gell_b200.cells as gc
+
+    cells = gc.lattice_spheroid(C5_CELLS, C5_N * LENGTH / 2, 5, LENGTH, C5_N)
+    gc.seed_ki67_states(cells, 13)
+    ref = rb.RefSim("c5", 38.0, 1e5, 0.1)
+    ref.set_cells(cells)
+    ref.prelod()
+    ref.lodsolver(C5_WARM)
+    a, b = rb.RefEvent("c5"), rb.RefEvent("c5")
+    ms = []
+    for _ in range(blocks):
+        ref.fm_update()
+        ref.prelod()
+        a.record()
+        ref.lodsolver(50)
+        b.record()
+        ms.append(a.elapsed_ms(b))
+    a.close()
+    b.close()
+    ref.close()
+    return {"ms_per_50_substeps": float(np.mean(ms)), "blocks": blocks,
+            "what": "the reference's LODsolver x 50 at 256^3 (oracle/_ref/libgellref_c5.so), same state as "
+                    "--workload c5"}
 
 
 def gpu_uuid_from_smi(index):
@@ -856,6 +922,8 @@ def main():
                          "against the plain solver at 256^3")
     ap.add_argument("--surrogate-weights", default=None, help="c5: weight file (default: the packaged one)")
     ap.add_argument("--no-conv-ring", action="store_true", help="c5: convolutions without the row ring")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="large: skip the short runs of the other workloads reported under components")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -886,6 +954,8 @@ def main():
         return
     line = run_gell(args, rank, world, local_rank)
     if rank == 0:
+        if world == 1 and not args.no_extras:
+            line["components"]["other_workloads"] = other_workloads(args, local_rank)
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)
