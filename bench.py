@@ -793,10 +793,16 @@ def run_reference(args, local_rank, world):
     sampler.start()
     time.sleep(0.3)
     ev = [rb.RefEvent("c2") for _ in range(2)]
+    se = [rb.RefEvent("c2") for _ in range(2)]
     K = args.steps
+    per_step = []
     ev[0].record()
     for _ in range(K):
+        # every facade ends in a device synchronisation, so these events do not perturb the steps
+        se[0].record()
         step()
+        se[1].record()
+        per_step.append(se[0].elapsed_ms(se[1]))
     ev[1].record()
     t_all = ev[0].elapsed_ms(ev[1])
     sampler.stop()
@@ -834,7 +840,7 @@ def run_reference(args, local_rank, world):
     t_e2e = ev[0].elapsed_ms(ev[1])
     alive_e2e = int(host.cells["sign"].sum())
     host.close()
-    for e in ev + pe:
+    for e in ev + pe + se:
         e.close()
     drug.close()
     o2.close()
@@ -856,7 +862,9 @@ def run_reference(args, local_rank, world):
         "components": {"cell_updates_per_s_fm_prelod": cnt[0] / (t_mech / 1e3),
                        "voxel_updates_per_s_lod": N ** 3 * NSUB * SUBSTEPS * K / (t_lod / 1e3),
                        "ms_fm_update": t_fm / K, "ms_prelod": t_pre / K, "ms_lod_10_substeps": t_lod / K,
-                       "lod_256cube_surrogate_workload": c5},
+                       "lod_256cube_surrogate_workload": c5,
+                       "ms_per_step_each": {"min": float(np.min(per_step)), "median": float(np.median(per_step)),
+                                            "max": float(np.max(per_step))}},
         "e2e": {"value": cnt[1] / (t_e2e / 1e3), "unit": "cell-updates/s", "steps": ke,
                 "h2d_bytes_per_step": int(ncell * 72), "d2h_bytes_per_step": int(ncell * 72)},
         "clocks": sampler.summary(),

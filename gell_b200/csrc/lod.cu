@@ -548,6 +548,49 @@ __global__ void __launch_bounds__(64 * kMaxComputeWarps, 1) k_sweep(const __grid
     }
 }
 
+// Results of group g of a tile straight from registers to the field, covering exactly the
+// elements a TMA store of the group's box writes (the tensor maps' extents: x boxes over (P, N*N),
+// y over (P, N, N), z over (P*N, N)).  y/z: one 128-byte row per element; x: each lane writes its
+// own line's 32 elements as eight 16-byte vectors (P is a multiple of 4).
+template <int AXIS>
+__device__ __forceinline__ void store_group_global(const LodArgs& a, const TileDesc& d, int g, int lane,
+                                                   const float o[32]) {
+    const int N = a.g.N, P = a.g.P;
+    float* p = a.sub[d.s].p;
+    const int j0 = 32 * g;
+    if (AXIS == 0) {
+        const long long line = (long long)d.c0 + lane;
+        if (line >= (long long)N * N) return;
+        float* row = p + line * P;
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (j0 + 4 * k < P)
+                *reinterpret_cast<float4*>(row + j0 + 4 * k) = make_float4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
+    } else if (AXIS == 1) {
+        const int x = d.c0 + lane;
+        if (x >= P) return;
+        float* col = p + x + (long long)d.c2 * a.g.PN + (long long)j0 * P;
+#pragma unroll
+        for (int e = 0; e < 32; ++e)
+            if (j0 + e < N) col[(long long)e * P] = o[e];
+    } else {
+        const long long pos = (long long)d.c0 + lane;
+        if (pos >= a.g.PN) return;
+        float* col = p + pos + (long long)j0 * a.g.PN;
+#pragma unroll
+        for (int e = 0; e < 32; ++e)
+            if (j0 + e < N) col[(long long)e * a.g.PN] = o[e];
+    }
+}
+
+// Back substitution of group g into o[] (the values backward_group leaves in the slot).
+template <int AXIS>
+__device__ __forceinline__ void backward_values(const SweepCtx& c, const SubDev& sd, float* slot, int g, int lane,
+                                                float& x, int exact, float o[32]) {
+    if ((sd.uni >> g) & 1u) backward_uniform<AXIS>(sd, slot, lane, x, o, exact);
+    else backward_full<AXIS>(c, slot, 32 * g, lane, x, o, exact);
+}
+
 // ------------------------------------------------------------------ ring sweeps
 //
 // The kernel above keeps a whole 32-line tile in shared memory from its forward elimination to its
@@ -562,11 +605,12 @@ __global__ void __launch_bounds__(64 * kMaxComputeWarps, 1) k_sweep(const __grid
 //   * back substitution takes the groups from the top down; a group below B-R is loaded again
 //     (the second read of the tile hits L2: the tile was read a few tens of microseconds before)
 //     and its Y values are recomputed from the checkpoint with the same operations, so they are
-//     bit-identical to the first pass; results go back to the field by TMA stores.
-// Each compute warp issues its own copies (lane 0), always into a slot whose previous occupant it
-// has finished with: loads run R (forward) or R-1 (back) groups ahead of their use.  Group g of a
-// tile of parity q lives in slot  g mod R  (q = 0) or  R-1 - (g mod R)  (q = 1), which makes the
-// slots the back substitution frees last the ones the next tile's first groups take.
+//     bit-identical to the first pass; results go from registers straight to the field (plain
+//     stores), so a group's slot is free as soon as its values are computed.
+// Each compute warp issues its own loads (lane 0), always into a slot whose previous occupant it
+// has finished with: loads run R groups ahead of their use.  Group g of a tile of parity q lives in
+// slot  g mod R  (q = 0) or  R-1 - (g mod R)  (q = 1), which makes the slots the back substitution
+// frees last the ones the next tile's first groups take.
 constexpr int kRingWarps = 8;
 constexpr int kRingMaxSlots = 8;
 
@@ -661,30 +705,15 @@ __device__ __forceinline__ bool ring_tile(const LodArgs& a, const TileDesc& d, c
             float Yh = ck[h * 32 + lane];
             forward(slot, h, Yh, true);  // the same Y values as the first pass
         }
-        backward_group<AXIS>(c, sd, slot, h, lane, x, a.exact);
-        // results in the slot: visible to the TMA store, then stored
+        float o[32];
+        backward_values<AXIS>(c, sd, slot, h, lane, x, a.exact, o);
+        store_group_global<AXIS>(a, d, h, lane, o);
+        // the slot is free once every lane is done with it: refill it at once (the recompute's
+        // stores into it must be ordered before the copy's writes)
         fence_proxy_async();
         __syncwarp();
-        if (lane == 0) {
-            box_store<AXIS>(a, d, h, slot);
-            bulk_commit();
-        }
-        if (h < B - 1) {
-            // the slot of group h+1: its store (one group ago) has read it by now
-            const int s1 = ring_slot(h + 1, q, R);
-            if (h + 1 >= R) {
-                if (lane == 0) bulk_wait_read<1>();
-                load(d, h + 1 - R, s1, false);  // back substitution's second read of group h+1-R
-            } else if (has_next) {
-                if (lane == 0) bulk_wait_read<1>();
-                load(dn, R - 2 - h, s1, R - 2 - h < keep);  // next tile (parity 1-q), group R-2-h
-            }
-        }
-        if (h == 0 && has_next) {
-            if (lane == 0) bulk_wait_read<0>();
-            load(dn, R - 1, s, R - 1 < keep);  // next tile, group R-1, into this group's slot
-        }
-        __syncwarp();
+        if (h >= R) load(d, h - R, s, false);                   // back substitution's second read of group h-R
+        else if (has_next) load(dn, R - 1 - h, s, R - 1 - h < keep);  // next tile (parity 1-q), group R-1-h
     }
     return true;
 }
