@@ -394,6 +394,10 @@ class Simulation:
         that many group slots per warp; False/0 = whole line tiles; -1 = automatic (the default)."""
         self._check(self.lib.gell_set_option(self.h, 5, int(on)), "gell_set_option")
 
+    def set_sweep_ring_lag(self, lag: int) -> None:
+        """Result stores a ring-sweep warp lets run before refilling a stored slot (0 = default)."""
+        self._check(self.lib.gell_set_option(self.h, 7, int(lag)), "gell_set_option")
+
     def set_sweep_l2hint(self, on: bool = True) -> None:
         """The ring sweeps' L2 eviction priorities (same results)."""
         self._check(self.lib.gell_set_option(self.h, 6, int(bool(on))), "gell_set_option")

@@ -113,5 +113,18 @@ template <int K>
 __device__ __forceinline__ void bulk_wait_read() {
     asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(K) : "memory");
 }
+// the same with a run-time count (0..7)
+__device__ __forceinline__ void bulk_wait_read_n(int k) {
+    switch (k) {
+        case 0: bulk_wait_read<0>(); break;
+        case 1: bulk_wait_read<1>(); break;
+        case 2: bulk_wait_read<2>(); break;
+        case 3: bulk_wait_read<3>(); break;
+        case 4: bulk_wait_read<4>(); break;
+        case 5: bulk_wait_read<5>(); break;
+        case 6: bulk_wait_read<6>(); break;
+        default: bulk_wait_read<7>(); break;
+    }
+}
 
 }  // namespace gell

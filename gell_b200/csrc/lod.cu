@@ -548,49 +548,6 @@ __global__ void __launch_bounds__(64 * kMaxComputeWarps, 1) k_sweep(const __grid
     }
 }
 
-// Results of group g of a tile straight from registers to the field, covering exactly the
-// elements a TMA store of the group's box writes (the tensor maps' extents: x boxes over (P, N*N),
-// y over (P, N, N), z over (P*N, N)).  y/z: one 128-byte row per element; x: each lane writes its
-// own line's 32 elements as eight 16-byte vectors (P is a multiple of 4).
-template <int AXIS>
-__device__ __forceinline__ void store_group_global(const LodArgs& a, const TileDesc& d, int g, int lane,
-                                                   const float o[32]) {
-    const int N = a.g.N, P = a.g.P;
-    float* p = a.sub[d.s].p;
-    const int j0 = 32 * g;
-    if (AXIS == 0) {
-        const long long line = (long long)d.c0 + lane;
-        if (line >= (long long)N * N) return;
-        float* row = p + line * P;
-#pragma unroll
-        for (int k = 0; k < 8; ++k)
-            if (j0 + 4 * k < P)
-                *reinterpret_cast<float4*>(row + j0 + 4 * k) = make_float4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
-    } else if (AXIS == 1) {
-        const int x = d.c0 + lane;
-        if (x >= P) return;
-        float* col = p + x + (long long)d.c2 * a.g.PN + (long long)j0 * P;
-#pragma unroll
-        for (int e = 0; e < 32; ++e)
-            if (j0 + e < N) col[(long long)e * P] = o[e];
-    } else {
-        const long long pos = (long long)d.c0 + lane;
-        if (pos >= a.g.PN) return;
-        float* col = p + pos + (long long)j0 * a.g.PN;
-#pragma unroll
-        for (int e = 0; e < 32; ++e)
-            if (j0 + e < N) col[(long long)e * a.g.PN] = o[e];
-    }
-}
-
-// Back substitution of group g into o[] (the values backward_group leaves in the slot).
-template <int AXIS>
-__device__ __forceinline__ void backward_values(const SweepCtx& c, const SubDev& sd, float* slot, int g, int lane,
-                                                float& x, int exact, float o[32]) {
-    if ((sd.uni >> g) & 1u) backward_uniform<AXIS>(sd, slot, lane, x, o, exact);
-    else backward_full<AXIS>(c, slot, 32 * g, lane, x, o, exact);
-}
-
 // ------------------------------------------------------------------ ring sweeps
 //
 // The kernel above keeps a whole 32-line tile in shared memory from its forward elimination to its
@@ -605,12 +562,14 @@ __device__ __forceinline__ void backward_values(const SweepCtx& c, const SubDev&
 //   * back substitution takes the groups from the top down; a group below B-R is loaded again
 //     (the second read of the tile hits L2: the tile was read a few tens of microseconds before)
 //     and its Y values are recomputed from the checkpoint with the same operations, so they are
-//     bit-identical to the first pass; results go from registers straight to the field (plain
-//     stores), so a group's slot is free as soon as its values are computed.
-// Each compute warp issues its own loads (lane 0), always into a slot whose previous occupant it
-// has finished with: loads run R groups ahead of their use.  Group g of a tile of parity q lives in
-// slot  g mod R  (q = 0) or  R-1 - (g mod R)  (q = 1), which makes the slots the back substitution
-// frees last the ones the next tile's first groups take.
+//     bit-identical to the first pass; results go back to the field by TMA stores.
+// Each compute warp issues its own copies (lane 0), always into a slot whose previous occupant it
+// has finished with.  A TMA store's read of its slot can take thousands of cycles to complete, so a
+// stored slot is refilled only L groups later (the warp waits for the store L groups back, never
+// the last one): forward loads run R groups ahead of their use, back-substitution loads R-L.
+// Group g of a tile of parity q lives in slot  g mod R  (q = 0) or  R-1 - (g mod R)  (q = 1),
+// which makes the slots the back substitution frees last the ones the next tile's first groups
+// take.
 constexpr int kRingWarps = 8;
 constexpr int kRingMaxSlots = 8;
 
@@ -630,8 +589,8 @@ __device__ __forceinline__ void ring_drain(uint64_t* full, uint32_t pend, uint32
 
 template <int AXIS, bool HINT>
 __device__ __forceinline__ bool ring_tile(const LodArgs& a, const TileDesc& d, const TileDesc& dn, bool has_next,
-                                          int q, int R, float* buf, uint64_t* full, float* ck, const float* sE,
-                                          int Na, uint32_t& phase, uint32_t& pend) {
+                                          int q, int R, int L, float* buf, uint64_t* full, float* ck,
+                                          const float* sE, int Na, uint32_t& phase, uint32_t& pend) {
     const int N = a.g.N;
     const int B = (N + 31) >> 5;
     const int keep = B - R;  // groups [keep, B) stay resident between the two passes
@@ -705,21 +664,39 @@ __device__ __forceinline__ bool ring_tile(const LodArgs& a, const TileDesc& d, c
             float Yh = ck[h * 32 + lane];
             forward(slot, h, Yh, true);  // the same Y values as the first pass
         }
-        float o[32];
-        backward_values<AXIS>(c, sd, slot, h, lane, x, a.exact, o);
-        store_group_global<AXIS>(a, d, h, lane, o);
-        // the slot is free once every lane is done with it: refill it at once (the recompute's
-        // stores into it must be ordered before the copy's writes)
+        backward_group<AXIS>(c, sd, slot, h, lane, x, a.exact);
+        // results in the slot: visible to the TMA store, then stored
         fence_proxy_async();
         __syncwarp();
-        if (h >= R) load(d, h - R, s, false);                   // back substitution's second read of group h-R
-        else if (has_next) load(dn, R - 1 - h, s, R - 1 - h < keep);  // next tile (parity 1-q), group R-1-h
+        if (lane == 0) {
+            box_store<AXIS>(a, d, h, slot);
+            bulk_commit();
+        }
+        // the slot of group h+L, stored L groups ago, is refilled once that store has read it: the L
+        // stores issued since may still be reading theirs
+        const int hl = h + L;
+        if (hl <= B - 1) {
+            if (hl >= R) {
+                if (lane == 0) bulk_wait_read_n(L);
+                load(d, hl - R, ring_slot(hl, q, R), false);  // back substitution's second read of group h+L-R
+            } else if (has_next) {
+                if (lane == 0) bulk_wait_read_n(L);
+                load(dn, R - 1 - hl, ring_slot(hl, q, R), R - 1 - hl < keep);  // next tile, group R-1-(h+L)
+            }
+        }
+        if (h == 0 && has_next) {
+            // the slots of groups L-1 .. 0 take the next tile's groups R-L .. R-1
+            if (lane == 0) bulk_wait_read_n(0);
+            for (int j = (L < B ? L : B) - 1; j >= 0; --j)
+                if (R - 1 - j >= 0) load(dn, R - 1 - j, ring_slot(j, q, R), R - 1 - j < keep);
+        }
+        __syncwarp();
     }
     return true;
 }
 
 template <int AXIS, bool HINT>
-__global__ void __launch_bounds__(32 * kRingWarps, 1) k_sweep_ring(const __grid_constant__ LodArgs a, int R) {
+__global__ void __launch_bounds__(32 * kRingWarps, 1) k_sweep_ring(const __grid_constant__ LodArgs a, int R, int L) {
     extern __shared__ __align__(1024) unsigned char sm[];
     const Geom g = a.g;
     const int N = g.N, P = g.P;
@@ -771,7 +748,7 @@ __global__ void __launch_bounds__(32 * kRingWarps, 1) k_sweep_ring(const __grid_
         const long long tn = t + step;
         const bool has_next = tn < total;
         const TileDesc dn = has_next ? tile_desc<AXIS>(a, tn, per_sub) : d;
-        if (!ring_tile<AXIS, HINT>(a, d, dn, has_next, k & 1, R, buf, fb, ck, sE, Na, phase, pend)) {
+        if (!ring_tile<AXIS, HINT>(a, d, dn, has_next, k & 1, R, L, buf, fb, ck, sE, Na, phase, pend)) {
             ring_drain(fb, pend, phase, R, a.err, lane);
             return;
         }
@@ -968,6 +945,9 @@ static gell_status lod_solver_ring(gell_ctx* c, const LodArgs& ax, const LodArgs
     }
     if (W < 1) return fail(c, GELL_ERR_UNSUPPORTED, "grid edge too large for the ring sweeps");
     const int smem = 1024 + W * R * kSlotFloats * 4 + align128(ns * Na * 4) + align128(W * B * 32 * 4) + W * R * 8;
+    // stores in flight per warp before a stored slot is refilled (1..R-1; a one-slot ring refills at once)
+    int L = c->sweep_ring_lag > 0 ? c->sweep_ring_lag : 3;
+    if (L > R - 1) L = R - 1;
     const bool hint = c->sweep_l2hint;
     const void* kx = hint ? (const void*)k_sweep_ring<0, true> : (const void*)k_sweep_ring<0, false>;
     const void* ky = hint ? (const void*)k_sweep_ring<1, true> : (const void*)k_sweep_ring<1, false>;
@@ -1008,13 +988,13 @@ static gell_status lod_solver_ring(gell_ctx* c, const LodArgs& ax, const LodArgs
     for (int k = 0; k < substeps; ++k) {
         GELL_KERNEL(c, "k_source_lines", k_source_lines<<<num_sms() * 8, 256, 0, c->stream>>>(sa));
         if (hint) {
-            GELL_KERNEL(c, "k_sweep_x", k_sweep_ring<0, true><<<gx, W * 32, smem, c->stream>>>(ax, R));
-            GELL_KERNEL(c, "k_sweep_y", k_sweep_ring<1, true><<<gy, W * 32, smem, c->stream>>>(ay, R));
-            GELL_KERNEL(c, "k_sweep_z", k_sweep_ring<2, true><<<gz, W * 32, smem, c->stream>>>(az, R));
+            GELL_KERNEL(c, "k_sweep_x", k_sweep_ring<0, true><<<gx, W * 32, smem, c->stream>>>(ax, R, L));
+            GELL_KERNEL(c, "k_sweep_y", k_sweep_ring<1, true><<<gy, W * 32, smem, c->stream>>>(ay, R, L));
+            GELL_KERNEL(c, "k_sweep_z", k_sweep_ring<2, true><<<gz, W * 32, smem, c->stream>>>(az, R, L));
         } else {
-            GELL_KERNEL(c, "k_sweep_x", k_sweep_ring<0, false><<<gx, W * 32, smem, c->stream>>>(ax, R));
-            GELL_KERNEL(c, "k_sweep_y", k_sweep_ring<1, false><<<gy, W * 32, smem, c->stream>>>(ay, R));
-            GELL_KERNEL(c, "k_sweep_z", k_sweep_ring<2, false><<<gz, W * 32, smem, c->stream>>>(az, R));
+            GELL_KERNEL(c, "k_sweep_x", k_sweep_ring<0, false><<<gx, W * 32, smem, c->stream>>>(ax, R, L));
+            GELL_KERNEL(c, "k_sweep_y", k_sweep_ring<1, false><<<gy, W * 32, smem, c->stream>>>(ay, R, L));
+            GELL_KERNEL(c, "k_sweep_z", k_sweep_ring<2, false><<<gz, W * 32, smem, c->stream>>>(az, R, L));
         }
     }
     return GELL_OK;

@@ -23,13 +23,14 @@ def bits_equal(a, b):
     return np.array_equal(np.asarray(a, np.float32).view(np.uint32), np.asarray(b, np.float32).view(np.uint32))
 
 
-def run(N, cells, field, k, ring, exact=False, warps=0, hint=False):
+def run(N, cells, field, k, ring, exact=False, warps=0, hint=False, lag=0):
     length = 10.0
     with gb.Simulation(voxel_num=N, voxel_length=length, max_cell_num=max(65536, len(cells) + 1024)) as sim:
         sim.add_substrate(gb.oxygen())
         sim.add_substrate(gb.drug())
         sim.set_sweep_ring(ring)
         sim.set_sweep_l2hint(hint)
+        sim.set_sweep_ring_lag(lag)
         sim.set_exact_chain(exact)
         if warps:
             sim.set_sweep_warps(warps)
@@ -87,11 +88,12 @@ def test_ring_sweeps_full_size_vs_oracle(N):
 
 @pytest.mark.parametrize("N", [131, 400])
 def test_ring_slot_counts_and_l2_hints_give_the_same_fields(N):
-    """Rings of 2, 3 and 5 slots (more groups loaded twice), with and without the L2 priorities."""
+    """Rings of 2, 3 and 5 slots (more groups loaded twice), with and without the L2 priorities,
+    with 1 to 4 result stores in flight per warp."""
     cells = one_per_voxel(N, 10.0, seed=N + 11, lo=N // 3, hi=N // 3 + N // 4)
     field = random_field(N, seed=N + 12)
     exp = oracle(N, cells, field, 2)
-    for ring, hint in ((2, False), (3, True), (5, False), (1, True)):
-        got = run(N, cells, field, 2, ring=ring, hint=hint)
+    for ring, hint, lag in ((2, False, 1), (3, True, 2), (5, False, 4), (1, True, 1), (1, False, 2), (4, False, 3)):
+        got = run(N, cells, field, 2, ring=ring, hint=hint, lag=lag)
         for sub in range(2):
-            assert bits_equal(got[sub], exp[sub]), (N, ring, hint, sub)
+            assert bits_equal(got[sub], exp[sub]), (N, ring, hint, lag, sub)
