@@ -398,10 +398,6 @@ class Simulation:
         """Result stores a ring-sweep warp lets run before refilling a stored slot (0 = default)."""
         self._check(self.lib.gell_set_option(self.h, 7, int(lag)), "gell_set_option")
 
-    def set_sweep_store(self, direct: bool) -> None:
-        """Line-tile sweeps: results by plain stores from registers (True) or TMA stores (False)."""
-        self._check(self.lib.gell_set_option(self.h, 8, int(bool(direct))), "gell_set_option")
-
     def set_sweep_l2hint(self, on: bool = True) -> None:
         """The ring sweeps' L2 eviction priorities (same results)."""
         self._check(self.lib.gell_set_option(self.h, 6, int(bool(on))), "gell_set_option")

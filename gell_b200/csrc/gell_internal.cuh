@@ -121,7 +121,6 @@ struct gell_ctx {
     int sweep_ring = -1;       // GELL_OPT_SWEEP_RING: -1 auto, 0 line tiles, 1 ring, >= 2 ring of at most that many slots
     bool sweep_l2hint = false;  // GELL_OPT_SWEEP_L2HINT: the ring sweeps' L2 eviction priorities
     int sweep_ring_lag = 0;     // GELL_OPT_SWEEP_RING_LAG: stores in flight per ring warp (0: default)
-    int sweep_store = 0;        // GELL_OPT_SWEEP_STORE: 0 TMA stores of the results, 1 plain stores
     bool sweeps_configured = false;  // the sweeps' shared-memory attribute is set on this device
     bool ring_configured = false;    // the same for the ring sweeps
 

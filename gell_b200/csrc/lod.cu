@@ -4,8 +4,8 @@
 // three Thomas sweeps LODkernel_x/y/z, each a launch of one thread per line.  Here a substep is
 // four launches, all substrates in each:
 //   k_source_lines  boundary layers + implicit uptake source on the x-lines that hold cells
-//   k_sweep<0, .>   boundary layers of the other lines + x sweep (x-lines are contiguous)
-//   k_sweep<1, .>   y sweep (element stride P)      k_sweep<2, .>  z sweep (element stride P*N)
+//   k_sweep<0>      boundary layers of the other lines + x sweep (x-lines are contiguous)
+//   k_sweep<1>      y sweep (element stride P)      k_sweep<2>  z sweep (element stride P*N)
 //
 // Streaming line tiles.  A warp owns a tile of 32 lines (one per lane) and walks its lane's line
 // out of shared memory.  The line is cut into B = ceil(N/32) groups of 32 elements; each group of
@@ -389,50 +389,6 @@ __device__ __forceinline__ void backward_group(const SweepCtx& c, const SubDev& 
     for (int b8 = 0; b8 < 4; ++b8) store8<AXIS>(slot, 8 * b8, lane, o + 8 * b8);
 }
 
-// Back substitution of group g into o[] (the values backward_group leaves in the slot).
-template <int AXIS>
-__device__ __forceinline__ void backward_values(const SweepCtx& c, const SubDev& sd, float* slot, int g, int lane,
-                                                float& x, int exact, float o[32]) {
-    if ((sd.uni >> g) & 1u) backward_uniform<AXIS>(sd, slot, lane, x, o, exact);
-    else backward_full<AXIS>(c, slot, 32 * g, lane, x, o, exact);
-}
-
-// Results of group g of a tile straight from registers to the field, covering exactly the
-// elements a TMA store of the group's box writes (the tensor maps' extents: x boxes over (P, N*N),
-// y over (P, N, N), z over (P*N, N)).  y/z: one 128-byte row per element; x: each lane writes its
-// own line's 32 elements as eight 16-byte vectors (P is a multiple of 4).  This takes the stores
-// off the TMA unit, which the loads keep busy.
-template <int AXIS>
-__device__ __forceinline__ void store_group_global(const LodArgs& a, const TileDesc& d, int g, int lane,
-                                                   const float o[32]) {
-    const int N = a.g.N, P = a.g.P;
-    float* p = a.sub[d.s].p;
-    const int j0 = 32 * g;
-    if (AXIS == 0) {
-        const long long line = (long long)d.c0 + lane;
-        if (line >= (long long)N * N) return;
-        float* row = p + line * P;
-#pragma unroll
-        for (int k = 0; k < 8; ++k)
-            if (j0 + 4 * k < P)
-                *reinterpret_cast<float4*>(row + j0 + 4 * k) = make_float4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
-    } else if (AXIS == 1) {
-        const int x = d.c0 + lane;
-        if (x >= P) return;
-        float* col = p + x + (long long)d.c2 * a.g.PN + (long long)j0 * P;
-#pragma unroll
-        for (int e = 0; e < 32; ++e)
-            if (j0 + e < N) col[(long long)e * P] = o[e];
-    } else {
-        const long long pos = (long long)d.c0 + lane;
-        if (pos >= a.g.PN) return;
-        float* col = p + pos + (long long)j0 * a.g.PN;
-#pragma unroll
-        for (int e = 0; e < 32; ++e)
-            if (j0 + e < N) col[(long long)e * a.g.PN] = o[e];
-    }
-}
-
 // y/z: rows of the end groups that hold boundary elements (j = 0 and j >= N-1) get b.
 template <int AXIS>
 __device__ __forceinline__ void edge_rows(const SweepCtx& c, float* slot, int g, int N, int lane) {
@@ -455,7 +411,7 @@ __device__ __forceinline__ void edge_rows(const SweepCtx& c, float* slot, int g,
 // group g of tile k.
 __host__ __device__ __forceinline__ int slot_index(int g, int q, int B) { return q ? B - 1 - g : g; }
 
-template <int AXIS, int Q, bool DS>
+template <int AXIS, int Q>
 __device__ __forceinline__ bool run_tile(const LodArgs& a, const TileDesc& d, float* buf, uint64_t* full,
                                          uint64_t* empty, const float* sEFR, int Na) {
     const int N = a.g.N;
@@ -487,19 +443,11 @@ __device__ __forceinline__ bool run_tile(const LodArgs& a, const TileDesc& d, fl
         else forward_group<AXIS>(c, slot, g, lane, Y, rs, xr);
     }
     float x = c.b;
-    if (DS) fence_proxy_async();  // the forward pass's writes to the slots, before their refills
     for (int g = B - 1; g >= 0; --g) {
         float* slot = buf + (size_t)slot_index(g, Q, B) * kSlotFloats;
-        if (DS) {
-            // results straight to the field; the slot is only read here, then handed back
-            float o[32];
-            backward_values<AXIS>(c, sd, slot, g, lane, x, a.exact, o);
-            store_group_global<AXIS>(a, d, g, lane, o);
-        } else {
-            backward_group<AXIS>(c, sd, slot, g, lane, x, a.exact);
-            // the slot now holds the results: make them visible to the TMA store, then hand it over
-            fence_proxy_async();
-        }
+        backward_group<AXIS>(c, sd, slot, g, lane, x, a.exact);
+        // the slot now holds the results: make them visible to the TMA store, then hand it over
+        fence_proxy_async();
         __syncwarp();
         if (lane == 0) mbar_arrive(empty + g);
     }
@@ -509,7 +457,7 @@ __device__ __forceinline__ bool run_tile(const LodArgs& a, const TileDesc& d, fl
 // The producer of compute warp w (lane 0 of warp W + w) follows the same tiles: first tile's loads,
 // then per signalled group the store of its results and the refill of the slot of the group before
 // it (whose store has read the slot by then), as the compute warp frees them.
-template <int AXIS, bool DS>
+template <int AXIS>
 __device__ void producer(const LodArgs& a, float* buf, uint64_t* full, uint64_t* empty, long long t, long long total,
                          long long step, long long per_sub) {
     const int B = (a.g.N + 31) >> 5;
@@ -526,12 +474,6 @@ __device__ void producer(const LodArgs& a, float* buf, uint64_t* full, uint64_t*
                 return;
             }
             float* slot = buf + (size_t)slot_index(g, Q, B) * kSlotFloats;
-            if (DS) {
-                // the compute warp stored the results itself: refill the slot with group B-1-g of
-                // the next tile (slot_index(B-1-g, 1-Q, B) == slot_index(g, Q, B))
-                if (has_next) box_load<AXIS>(a, dn, B - 1 - g, slot, full + (B - 1 - g));
-                continue;
-            }
             box_store<AXIS>(a, d, g, slot);
             bulk_commit();
             if (has_next && g + 1 <= B - 1) {
@@ -542,10 +484,8 @@ __device__ void producer(const LodArgs& a, float* buf, uint64_t* full, uint64_t*
             }
         }
         if (!has_next) break;
-        if (!DS) {
-            bulk_wait_read<0>();
-            box_load<AXIS>(a, dn, B - 1, buf + (size_t)slot_index(0, Q, B) * kSlotFloats, full + (B - 1));
-        }
+        bulk_wait_read<0>();
+        box_load<AXIS>(a, dn, B - 1, buf + (size_t)slot_index(0, Q, B) * kSlotFloats, full + (B - 1));
         t = tn;
         d = dn;
     }
@@ -555,7 +495,7 @@ __device__ void producer(const LodArgs& a, float* buf, uint64_t* full, uint64_t*
 
 // blockDim = 2W warps: W <= kMaxComputeWarps compute warps, then their W producer warps.
 constexpr int kMaxComputeWarps = 4;
-template <int AXIS, bool DS>
+template <int AXIS>
 __global__ void __launch_bounds__(64 * kMaxComputeWarps, 1) k_sweep(const __grid_constant__ LodArgs a) {
     extern __shared__ __align__(1024) unsigned char sm[];
     const Geom g = a.g;
@@ -593,8 +533,7 @@ __global__ void __launch_bounds__(64 * kMaxComputeWarps, 1) k_sweep(const __grid
         const int w = warp - W;
         const long long t = (long long)blockIdx.x * W + w;
         if (lane == 0 && t < total)
-            producer<AXIS, DS>(a, slots + (size_t)w * B * kSlotFloats, full + w * 32, empty + w * 32, t, total, step,
-                               per_sub);
+            producer<AXIS>(a, slots + (size_t)w * B * kSlotFloats, full + w * 32, empty + w * 32, t, total, step, per_sub);
         return;
     }
     float* buf = slots + (size_t)warp * B * kSlotFloats;
@@ -603,8 +542,8 @@ __global__ void __launch_bounds__(64 * kMaxComputeWarps, 1) k_sweep(const __grid
     int k = 0;
     for (long long t = (long long)blockIdx.x * W + warp; t < total; t += step, ++k) {
         const TileDesc d = tile_desc<AXIS>(a, t, per_sub);
-        const bool ok = (k & 1) ? run_tile<AXIS, 1, DS>(a, d, buf, fb, eb, sEFR, Na)
-                                : run_tile<AXIS, 0, DS>(a, d, buf, fb, eb, sEFR, Na);
+        const bool ok = (k & 1) ? run_tile<AXIS, 1>(a, d, buf, fb, eb, sEFR, Na)
+                                : run_tile<AXIS, 0>(a, d, buf, fb, eb, sEFR, Na);
         if (!ok) break;
     }
 }
@@ -1110,10 +1049,9 @@ gell_status lod_solver(gell_ctx* c, int sub, int substeps) {
     // the shared-memory opt-in is a per-device function attribute: set once per context (each
     // context lives on one device)
     if (!c->sweeps_configured) {
-        for (const void* k : {(const void*)k_sweep<0, false>, (const void*)k_sweep<1, false>,
-                              (const void*)k_sweep<2, false>, (const void*)k_sweep<0, true>,
-                              (const void*)k_sweep<1, true>, (const void*)k_sweep<2, true>})
-            GELL_CUDA(c, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
+        GELL_CUDA(c, cudaFuncSetAttribute(k_sweep<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
+        GELL_CUDA(c, cudaFuncSetAttribute(k_sweep<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
+        GELL_CUDA(c, cudaFuncSetAttribute(k_sweep<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
         c->sweeps_configured = true;
     }
     const long long xt = ((long long)N * N + 31) / 32 * ns;
@@ -1131,10 +1069,8 @@ gell_status lod_solver(gell_ctx* c, int sub, int substeps) {
         long long cap = (long long)num_sms() * occ;
         return (int)(want < cap ? want : cap);
     };
-    const bool ds = c->sweep_store == 1;
-    const int gx = grid(xt, ds ? (const void*)k_sweep<0, true> : (const void*)k_sweep<0, false>),
-              gy = grid(yt, ds ? (const void*)k_sweep<1, true> : (const void*)k_sweep<1, false>),
-              gz = grid(zt, ds ? (const void*)k_sweep<2, true> : (const void*)k_sweep<2, false>);
+    const int gx = grid(xt, (const void*)k_sweep<0>), gy = grid(yt, (const void*)k_sweep<1>),
+              gz = grid(zt, (const void*)k_sweep<2>);
     SrcArgs sa{};
     for (int s = s0; s < s1; ++s) {
         const Substrate& S = c->subs[s];
@@ -1149,15 +1085,9 @@ gell_status lod_solver(gell_ctx* c, int sub, int substeps) {
     sa.dt = c->P.diffusion_dt;
     for (int k = 0; k < substeps; ++k) {
         GELL_KERNEL(c, "k_source_lines", k_source_lines<<<num_sms() * 8, 256, 0, c->stream>>>(sa));
-        if (ds) {
-            GELL_KERNEL(c, "k_sweep_x", k_sweep<0, true><<<gx, w * 64, smem, c->stream>>>(ax));
-            GELL_KERNEL(c, "k_sweep_y", k_sweep<1, true><<<gy, w * 64, smem, c->stream>>>(ay));
-            GELL_KERNEL(c, "k_sweep_z", k_sweep<2, true><<<gz, w * 64, smem, c->stream>>>(az));
-        } else {
-            GELL_KERNEL(c, "k_sweep_x", k_sweep<0, false><<<gx, w * 64, smem, c->stream>>>(ax));
-            GELL_KERNEL(c, "k_sweep_y", k_sweep<1, false><<<gy, w * 64, smem, c->stream>>>(ay));
-            GELL_KERNEL(c, "k_sweep_z", k_sweep<2, false><<<gz, w * 64, smem, c->stream>>>(az));
-        }
+        GELL_KERNEL(c, "k_sweep_x", k_sweep<0><<<gx, w * 64, smem, c->stream>>>(ax));
+        GELL_KERNEL(c, "k_sweep_y", k_sweep<1><<<gy, w * 64, smem, c->stream>>>(ay));
+        GELL_KERNEL(c, "k_sweep_z", k_sweep<2><<<gz, w * 64, smem, c->stream>>>(az));
     }
     return GELL_OK;
 }

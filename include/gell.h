@@ -284,8 +284,7 @@ enum {
     GELL_OPT_CONV_RING = 4,
     GELL_OPT_SWEEP_RING = 5,
     GELL_OPT_SWEEP_L2HINT = 6,
-    GELL_OPT_SWEEP_RING_LAG = 7,
-    GELL_OPT_SWEEP_STORE = 8
+    GELL_OPT_SWEEP_RING_LAG = 7
 };
 /* GELL_OPT_SWEEP_RING (-1..8, default -1): 1 runs the LOD sweeps as ring kernels (a few group
  * slots of shared memory per warp; back substitution re-reads each group from L2 and recomputes its
@@ -295,9 +294,7 @@ enum {
  * GELL_OPT_SWEEP_L2HINT (0 or 1, default 0): the ring sweeps load groups they will read again with
  * priority to stay in L2.  GELL_OPT_SWEEP_RING_LAG (0..7, default 0 = 3): how many of its own
  * result stores a ring warp lets run before it refills a stored slot (capped at the slots less
- * one).  GELL_OPT_SWEEP_STORE (0 or 1, default 0): 1 makes the line-tile sweeps write their
- * results from registers with plain stores instead of TMA stores from shared memory.  Results are
- * identical for every value of these options. */
+ * one).  Results are identical for every value of these options. */
 /* GELL_OPT_CONV_RING (0 or 1, default 1): the surrogate's convolutions keep the input rows of
  * consecutive lines in a ring of shared-memory slots (each row read from L2 once per unit of 32
  * lines) instead of loading all nine rows per tile; the results are the same. */

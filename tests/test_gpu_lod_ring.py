@@ -97,26 +97,3 @@ def test_ring_slot_counts_and_l2_hints_give_the_same_fields(N):
         got = run(N, cells, field, 2, ring=ring, hint=hint, lag=lag)
         for sub in range(2):
             assert bits_equal(got[sub], exp[sub]), (N, ring, hint, lag, sub)
-
-
-@pytest.mark.parametrize("N", [32, 37, 131, 400])
-def test_line_tiles_with_plain_result_stores_bit_exact(N):
-    """GELL_OPT_SWEEP_STORE = 1: the line-tile sweeps write results from registers with plain stores
-    (the same elements a TMA store of each box covers, padding columns included)."""
-    cells = one_per_voxel(N, 10.0, seed=N + 21, lo=N // 4, hi=N // 4 + N // 3)
-    field = random_field(N, seed=N + 22)
-    length = 10.0
-    with gb.Simulation(voxel_num=N, voxel_length=length, max_cell_num=max(65536, len(cells) + 1024)) as sim:
-        sim.add_substrate(gb.oxygen())
-        sim.add_substrate(gb.drug())
-        sim.set_sweep_ring(0)
-        sim.set_sweep_store(True)
-        sim.set_field(0, field)
-        sim.set_field(1, field * np.float32(0.03))
-        sim.import_cells(cells)
-        sim.PreLOD()
-        sim.LODsolver(3)
-        got = (sim.field(0), sim.field(1))
-    exp = oracle(N, cells, field, 3)
-    for sub in range(2):
-        assert bits_equal(got[sub], exp[sub]), (N, sub)
