@@ -946,7 +946,7 @@ static gell_status lod_solver_ring(gell_ctx* c, const LodArgs& ax, const LodArgs
     if (W < 1) return fail(c, GELL_ERR_UNSUPPORTED, "grid edge too large for the ring sweeps");
     const int smem = 1024 + W * R * kSlotFloats * 4 + align128(ns * Na * 4) + align128(W * B * 32 * 4) + W * R * 8;
     // stores in flight per warp before a stored slot is refilled (1..R-1; a one-slot ring refills at once)
-    int L = c->sweep_ring_lag > 0 ? c->sweep_ring_lag : 3;
+    int L = c->sweep_ring_lag > 0 ? c->sweep_ring_lag : 1;
     if (L > R - 1) L = R - 1;
     const bool hint = c->sweep_l2hint;
     const void* kx = hint ? (const void*)k_sweep_ring<0, true> : (const void*)k_sweep_ring<0, false>;

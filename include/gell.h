@@ -292,7 +292,7 @@ enum {
  * tiles; 2..8 do the same with at most that many slots per warp; 0 keeps whole line tiles in shared
  * memory; -1 picks the ring when fewer than four line tiles fit per SM (long lines, N > 416).
  * GELL_OPT_SWEEP_L2HINT (0 or 1, default 0): the ring sweeps load groups they will read again with
- * priority to stay in L2.  GELL_OPT_SWEEP_RING_LAG (0..7, default 0 = 3): how many of its own
+ * priority to stay in L2.  GELL_OPT_SWEEP_RING_LAG (0..7, default 0 = 1): how many of its own
  * result stores a ring warp lets run before it refills a stored slot (capped at the slots less
  * one).  Results are identical for every value of these options. */
 /* GELL_OPT_CONV_RING (0 or 1, default 1): the surrogate's convolutions keep the input rows of
