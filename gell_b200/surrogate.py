@@ -195,14 +195,17 @@ def train(N: int = 256, pairs: int = 2000, substeps: int = 50, rate_scale: float
 
 
 def calibrate(sw: SurrogateWeights, N: int = 256, pairs: int = 64, seed: int = 1234,
-              cells: tuple[int, int] = (150_000, 450_000), tol: float = 0.01, log=print):
+              cells: tuple[int, int] = (150_000, 450_000), tol: float = 0.01, log=print,
+              warm: tuple[int, int] = (300, 1000), moves: tuple[int, int] = (1, 5), margin: float = 1.0):
     """Run the library's operator and judge on held-out pairs and set the threshold: the judge's
     residual r bounds the error e (L-infinity inside the shell, units of the boundary value) on
-    these pairs as e <= kappa * r with kappa the largest ratio seen; threshold = tol / kappa.
-    Returns (threshold, [(r, e)])."""
+    these pairs as e <= kappa * r with kappa the largest ratio seen; threshold = tol / (kappa *
+    margin).  `warm` and `moves` choose the pairs' regime (see PairSource): fields relaxed for
+    800-1500 substeps with one mechanics step per block are the quasi-steady fields the surrogate
+    stands in for.  Returns (threshold, [(r, e)])."""
     import gell_b200 as gb
 
-    src = PairSource(N, cells, seed, sw.substeps)
+    src = PairSource(N, cells, seed, sw.substeps, warm=warm, moves=moves)
     b = sim_boundary(gb)
     inner = ~shell_mask(N)
     out = []
@@ -225,7 +228,7 @@ def calibrate(sw: SurrogateWeights, N: int = 256, pairs: int = 64, seed: int = 1
     finally:
         src.close()
     kappa = max(e / max(r, 1e-12) for r, e in out)
-    thr = tol / kappa
+    thr = tol / (kappa * margin)
     log(f"calibration: kappa {kappa:.3g}, threshold {thr:.3e}, accepted {sum(r <= thr for r, _ in out)}/{len(out)}")
     return thr, out
 
@@ -302,6 +305,28 @@ def main(argv=None) -> int:
         tp.add_argument("--reps", type=int, default=2)
         t = tp.parse_args(argv[1:])
         time_training(t.N, t.reps)
+        return 0
+    if argv and argv[0] == "calibrate":
+        cp = argparse.ArgumentParser(description="Recalibrate the judge of a weight file on held-out pairs "
+                                                 "(`... calibrate --weights IN --out OUT`).")
+        cp.add_argument("--weights", default=DEFAULT_WEIGHTS)
+        cp.add_argument("--out", required=True)
+        cp.add_argument("--N", type=int, default=256)
+        cp.add_argument("--pairs", type=int, default=64)
+        cp.add_argument("--seed", type=int, default=4321)
+        cp.add_argument("--warm", type=int, nargs=2, default=(800, 1500))
+        cp.add_argument("--moves", type=int, nargs=2, default=(1, 1))
+        cp.add_argument("--cells", type=int, nargs=2, default=(150_000, 450_000))
+        cp.add_argument("--margin", type=float, default=1.1)
+        cp.add_argument("--tol", type=float, default=0.01)
+        c = cp.parse_args(argv[1:])
+        sw = load_weights(c.weights)
+        t1 = time.time()
+        sw.threshold, pts = calibrate(sw, c.N, c.pairs, c.seed, tuple(c.cells), c.tol,
+                                      log=lambda m: print(m, flush=True), warm=tuple(c.warm), moves=tuple(c.moves),
+                                      margin=c.margin)
+        print(f"calibration: {c.pairs} pairs in {time.time() - t1:.1f} s", flush=True)
+        save_weights(c.out, sw)
         return 0
     if argv and argv[0] == "fit":
         argv = argv[1:]
