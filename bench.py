@@ -637,6 +637,56 @@ def run_c4(args, rank, world, local_rank):
     return line
 
 
+# ---------------------------------------------------------------------------- LOD only
+
+def run_lod(args, rank, world, local_rank):
+    """--workload lod: LOD substeps alone on an N^3 grid (--lod-n) with one or two substrates
+    (--lod-subs) and a 10^6-cell lattice spheroid's uptake map; K timed substeps.  For kernel studies
+    of the sweeps at other sizes than the headline's (the line tiles or, for N > 416, the ring
+    kernels, as the library picks them)."""
+    import torch
+    import gell_b200 as gb
+
+    torch.cuda.set_device(local_rank)
+    n_lod = args.lod_n
+    cells = gb.lattice_spheroid(NCELLS, n_lod * LENGTH / 2, 0, LENGTH, n_lod)
+    sim = gb.Simulation(voxel_num=n_lod, voxel_length=LENGTH, max_cell_num=NCELLS + 1024)
+    sim.add_substrate(gb.oxygen())
+    if args.lod_subs > 1:
+        sim.add_substrate(gb.drug())
+    stream = torch.cuda.Stream()
+    sim.set_stream(stream)
+    sim.import_cells(cells)
+    sim.PreLOD()
+    sim.LODsolver(args.warmup)
+    sim.sync()
+    K = args.steps
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.LODsolver(K)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1)
+    sim.profile(True)
+    sim.profile_read(reset=True)
+    sim.LODsolver(max(1, min(K, 10)))
+    sim.sync()
+    prof = sim.profile_read(reset=True)
+    sim.profile(False)
+    sim.close()
+    peak, peak_kind = hbm_peak()
+    per_launch = 8.0 * n_lod ** 3 * args.lod_subs
+    kern = {k: {"avg_ms": v[1] / v[0], "achieved_gbs": per_launch / (v[1] / v[0] / 1e3) / 1e9,
+                "frac": per_launch / (v[1] / v[0] / 1e3) / 1e9 / peak}
+            for k, v in prof.items() if k.startswith("k_sweep")}
+    return {"metric": "voxel-updates/s (LOD substeps alone)", "value": n_lod ** 3 * args.lod_subs * K / (t / 1e3),
+            "unit": "voxel-updates/s", "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": t / K,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: uptake map of a seeded 10^6-cell lattice spheroid, fields at the boundary values",
+            "config": {"workload": f"LOD substeps, {n_lod}^3 voxels x {args.lod_subs} substrate(s)"},
+            "kernels": kern, "peak": {"hbm_gbs": peak, "source": peak_kind}}
+
+
 # ---------------------------------------------------------------------------- other workloads
 
 def other_workloads(args, local_rank):
@@ -924,12 +974,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("gell", "reference"), default="gell")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=("large", "c3", "c4", "c5"), default="large",
+    ap.add_argument("--workload", choices=("large", "c3", "c4", "c5", "lod"), default="large",
                     help="large: 400^3, 10^6 cells (the headline line); c3: 600^3, 5*10^6 cells with "
                          "birth/death; c4: ensemble of 64 small instances; c5: the learned oxygen surrogate "
-                         "against the plain solver at 256^3")
+                         "against the plain solver at 256^3; lod: LOD substeps alone (--lod-n, --lod-subs)")
     ap.add_argument("--surrogate-weights", default=None, help="c5: weight file (default: the packaged one)")
     ap.add_argument("--no-conv-ring", action="store_true", help="c5: convolutions without the row ring")
+    ap.add_argument("--lod-n", type=int, default=400, help="lod: grid edge")
+    ap.add_argument("--lod-subs", type=int, choices=(1, 2), default=2, help="lod: substrates")
     ap.add_argument("--no-extras", action="store_true",
                     help="large: skip the short runs of the other workloads reported under components")
     args = ap.parse_args()
@@ -952,8 +1004,8 @@ def main():
         import torch.distributed as td
         torch.cuda.set_device(local_rank)
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    if args.workload in ("c3", "c4", "c5"):
-        line = {"c3": run_c3, "c4": run_c4, "c5": run_c5}[args.workload](args, rank, world, local_rank)
+    if args.workload in ("c3", "c4", "c5", "lod"):
+        line = {"c3": run_c3, "c4": run_c4, "c5": run_c5, "lod": run_lod}[args.workload](args, rank, world, local_rank)
         if rank == 0:
             print(json.dumps(line), flush=True)
         if world > 1:
