@@ -130,6 +130,8 @@ def load_library() -> ctypes.CDLL:
     L.gell_ensemble_run_mechanics.argtypes = [P, ctypes.c_int, ctypes.c_int]
     L.gell_ensemble_tune.argtypes = [P, ctypes.c_int, P, P, P]
     L.gell_ensemble_sync.argtypes = [P]
+    L.gell_ensemble_set_batched.argtypes = [P, ctypes.c_int]
+    L.gell_ensemble_get_batched.argtypes = [P, P]
     L.gell_field_import.argtypes = [P, ctypes.c_int, P, ctypes.c_int]
     L.gell_field_export.argtypes = [P, ctypes.c_int, P, ctypes.c_int]
     L.gell_fm_update.argtypes = [P]
@@ -173,7 +175,7 @@ def load_library() -> ctypes.CDLL:
                  "gell_save_field_slice_csv", "gell_checkpoint_save", "gell_checkpoint_load",
                  "gell_reference_spheroid", "gell_ensemble_create", "gell_ensemble_destroy",
                  "gell_ensemble_configure", "gell_ensemble_run_mechanics", "gell_ensemble_tune",
-                 "gell_ensemble_sync", "gell_surrogate_load", "gell_lod_surrogate", "gell_surrogate_infer",
+                 "gell_ensemble_sync", "gell_ensemble_set_batched", "gell_ensemble_get_batched", "gell_surrogate_load", "gell_lod_surrogate", "gell_surrogate_infer",
                  "gell_surrogate_run_layers", "gell_surrogate_read", "gell_surrogate_train_init",
                  "gell_surrogate_train_pair", "gell_surrogate_train_read"):
         getattr(L, name).restype = ctypes.c_int
@@ -549,6 +551,15 @@ class Ensemble:
         self._check(self.lib.gell_ensemble_tune(self.h, substeps, ctypes.byref(t), ctypes.byref(b), ctypes.byref(w)),
                     "gell_ensemble_tune")
         return t.value, b.value, w.value
+
+    def set_batched(self, on: bool = True) -> None:
+        """LOD substeps of all members as one launch per sweep (same results)."""
+        self._check(self.lib.gell_ensemble_set_batched(self.h, int(bool(on))), "gell_ensemble_set_batched")
+
+    def batched(self) -> bool:
+        v = ctypes.c_int()
+        self._check(self.lib.gell_ensemble_get_batched(self.h, ctypes.byref(v)), "gell_ensemble_get_batched")
+        return bool(v.value)
 
     def sync(self) -> None:
         self._check(self.lib.gell_ensemble_sync(self.h), "gell_ensemble_sync")

@@ -7,6 +7,11 @@
 // leave mostly idle.  The graph is replayed for every pair of steps and captured again when a
 // member's cell count, substrates or double-buffer assignment, or the substep count, changed.
 // gell_ensemble_tune times a few branch counts and sweep tile widths and keeps the fastest.
+//
+// Batched LOD (gell_ensemble_set_batched, or chosen by the tuner): each captured step is every
+// member's FM_update and PreLOD on the branches, then the LOD substeps of ALL members as one
+// launch per sweep axis (and one for the uptake source) over a device-side work list of every
+// member's line tiles (gell::lod_batch_run), instead of four launches per member and substep.
 #include <initializer_list>
 #include <vector>
 
@@ -20,9 +25,11 @@ struct gell_ensemble {
     std::vector<cudaEvent_t> join, ready;
     int branches = 0;     // branch streams in use
     int sweep_warps = 0;  // GELL_OPT_SWEEP_WARPS given to every member (0 = each member's default)
+    bool batched = false;  // LOD substeps of all members as one launch per sweep (gell::lod_batch_run)
+    gell::LodBatch* batch = nullptr;
     cudaGraphExec_t exec = nullptr;
     // what the graph was captured for
-    int key_substeps = -1, key_branches = -1, key_warps = -1;
+    int key_substeps = -1, key_branches = -1, key_warps = -1, key_batched = -1;
     std::vector<int> key_n, key_nsub;
     std::vector<uint32_t> key_par;
     std::vector<long long> launches;  // kernels per member in one replay
@@ -33,7 +40,8 @@ namespace {
 constexpr int kMaxBranches = 64;
 
 bool key_matches(const gell_ensemble* e, int substeps) {
-    if (!e->exec || e->key_substeps != substeps || e->key_branches != e->branches || e->key_warps != e->sweep_warps)
+    if (!e->exec || e->key_substeps != substeps || e->key_branches != e->branches || e->key_warps != e->sweep_warps ||
+        e->key_batched != (int)e->batched)
         return false;
     for (size_t i = 0; i < e->m.size(); ++i) {
         const gell_ctx* c = e->m[i];
@@ -57,19 +65,33 @@ gell_status capture(gell_ensemble* e, int substeps) {
         saved[i] = e->m[i]->stream;
         l0[i] = e->m[i]->launches;
     }
+    if (e->batched) {
+        // the work list of every member's substrates, built outside the capture
+        gell::lod_batch_free(e->batch);
+        e->batch = nullptr;
+        if (gell_status bs = gell::lod_batch_build(e->m, &e->batch)) return bs;
+    }
     if (cudaStreamBeginCapture(e->origin, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return GELL_ERR_CUDA;
     gell_status st = GELL_OK;
-    cudaError_t ce = cudaEventRecord(e->fork, e->origin);
-    for (int b = 0; b < nb && ce == cudaSuccess; ++b) ce = cudaStreamWaitEvent(e->pool[b], e->fork, 0);
-    for (size_t i = 0; i < n && ce == cudaSuccess && st == GELL_OK; ++i) {
-        gell_ctx* c = e->m[i];
-        c->stream = e->pool[i % nb];
-        st = gell::one_mechanics_step(c, substeps);
-        if (st == GELL_OK) st = gell::one_mechanics_step(c, substeps);
-    }
-    for (int b = 0; b < nb && ce == cudaSuccess; ++b) {
-        ce = cudaEventRecord(e->join[b], e->pool[b]);
-        if (ce == cudaSuccess) ce = cudaStreamWaitEvent(e->origin, e->join[b], 0);
+    cudaError_t ce = cudaSuccess;
+    // batched: per step, every member's mechanics (FM_update, PreLOD) on the branches, joined, then
+    // all members' LOD substeps as one launch per sweep on the origin stream; otherwise each member's
+    // two whole steps on its branch
+    const int rounds = e->batched ? 2 : 1;
+    for (int r = 0; r < rounds && ce == cudaSuccess && st == GELL_OK; ++r) {
+        ce = cudaEventRecord(e->fork, e->origin);
+        for (int b = 0; b < nb && ce == cudaSuccess; ++b) ce = cudaStreamWaitEvent(e->pool[b], e->fork, 0);
+        for (size_t i = 0; i < n && ce == cudaSuccess && st == GELL_OK; ++i) {
+            gell_ctx* c = e->m[i];
+            c->stream = e->pool[i % nb];
+            st = gell::one_mechanics_step(c, e->batched ? 0 : substeps);
+            if (st == GELL_OK && !e->batched) st = gell::one_mechanics_step(c, substeps);
+        }
+        for (int b = 0; b < nb && ce == cudaSuccess; ++b) {
+            ce = cudaEventRecord(e->join[b], e->pool[b]);
+            if (ce == cudaSuccess) ce = cudaStreamWaitEvent(e->origin, e->join[b], 0);
+        }
+        if (e->batched && ce == cudaSuccess && st == GELL_OK) st = gell::lod_batch_run(e->batch, e->origin, substeps);
     }
     cudaGraph_t g = nullptr;
     const cudaError_t ee = cudaStreamEndCapture(e->origin, &g);
@@ -94,6 +116,7 @@ gell_status capture(gell_ensemble* e, int substeps) {
     e->key_substeps = substeps;
     e->key_branches = nb;
     e->key_warps = e->sweep_warps;
+    e->key_batched = (int)e->batched;
     for (size_t i = 0; i < n; ++i) {
         e->key_n[i] = e->m[i]->n;
         e->key_nsub[i] = (int)e->m[i]->subs.size();
@@ -175,6 +198,7 @@ gell_status gell_ensemble_destroy(gell_ensemble* e) {
         if (v) cudaEventDestroy(v);
     for (auto v : e->ready)
         if (v) cudaEventDestroy(v);
+    gell::lod_batch_free(e->batch);
     if (e->fork) cudaEventDestroy(e->fork);
     if (e->done) cudaEventDestroy(e->done);
     if (e->origin) cudaStreamDestroy(e->origin);
@@ -188,6 +212,18 @@ gell_status gell_ensemble_configure(gell_ensemble* e, int branches, int sweep_wa
     e->branches = branches < nb ? branches : nb;
     e->sweep_warps = sweep_warps;
     apply_warps(e);
+    return GELL_OK;
+}
+
+gell_status gell_ensemble_set_batched(gell_ensemble* e, int on) {
+    if (!e) return GELL_ERR_INVALID_ARG;
+    e->batched = on != 0;
+    return GELL_OK;
+}
+
+gell_status gell_ensemble_get_batched(const gell_ensemble* e, int* on) {
+    if (!e || !on) return GELL_ERR_INVALID_ARG;
+    *on = e->batched ? 1 : 0;
     return GELL_OK;
 }
 
@@ -254,8 +290,12 @@ gell_status gell_ensemble_tune(gell_ensemble* e, int substeps, int* steps_taken,
     if (cudaEventCreate(&t0) != cudaSuccess || cudaEventCreate(&t1) != cudaSuccess) return GELL_ERR_CUDA;
     float best = 3.4e38f;
     int bb = e->branches, bw = e->sweep_warps;
+    bool bbat = e->batched;
     gell_status st = GELL_OK;
-    for (int w : {0, 2, 1}) {
+    for (int v = 0; v < 4; ++v) {
+        // line-tile widths 0, 2, 1 with per-member sweeps, then the batched sweeps
+        const int w = v == 1 ? 2 : (v == 2 ? 1 : 0);
+        e->batched = v == 3;
         for (int b = 1; st == GELL_OK; b *= 2) {
             const int br = b < nb ? b : nb;
             e->branches = br;
@@ -278,6 +318,7 @@ gell_status gell_ensemble_tune(gell_ensemble* e, int substeps, int* steps_taken,
                     best = ms;
                     bb = br;
                     bw = w;
+                    bbat = e->batched;
                 }
                 st = scatter(e);
             }
@@ -292,6 +333,7 @@ gell_status gell_ensemble_tune(gell_ensemble* e, int substeps, int* steps_taken,
     }
     e->branches = bb;
     e->sweep_warps = bw;
+    e->batched = bbat;
     apply_warps(e);
     for (gell_ctx* c : e->m)
         if (gell_status s2 = gell::cells_end(c, GELL_OK)) return s2;

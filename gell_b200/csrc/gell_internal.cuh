@@ -266,6 +266,13 @@ inline int blocks_for(long long n, int threads) {
 
 // ------------------------------------------------------------------ entry points between files
 gell_status lod_solver(gell_ctx* c, int sub, int substeps);
+// LOD substeps of many contexts at once (ensembles): one launch per sweep axis over every member's
+// line tiles.  build allocates the device work list (outside any stream capture); run queues
+// `substeps` substeps of every member on `st`.
+struct LodBatch;
+gell_status lod_batch_build(const std::vector<gell_ctx*>& members, LodBatch** out);
+gell_status lod_batch_run(LodBatch* b, cudaStream_t st, int substeps);
+void lod_batch_free(LodBatch* b);
 gell_status prelod(gell_ctx* c, int sub);
 gell_status fm_update(gell_ctx* c);
 gell_status selftest_timeout(gell_ctx* c, int polls);

@@ -29,6 +29,9 @@
 // division (checked against it by gell_selftest_division and by the bit-exact parity tests).
 #include <cuda.h>
 
+#include <cstring>
+#include <vector>
+
 #include "async_copy.cuh"
 #include "gell_internal.cuh"
 
@@ -759,6 +762,281 @@ __global__ void __launch_bounds__(32 * kRingWarps, 1) k_sweep_ring(const __grid_
     if (lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
 
+// ------------------------------------------------------------------ batched sweeps (ensembles)
+//
+// One launch per axis sweeps the lines of MANY grids: every (member, substrate) pair of an
+// ensemble is an item with its own geometry, tensor maps and Thomas tables, and the items' line
+// tiles form one list that the persistent CTAs walk (warp w of CTA b takes tiles b*W + w + k*step).
+// The line-tile pipeline is the one above (a producer lane per compute warp, whole tiles in
+// shared memory), with two changes for tiles of different lengths (B groups, up to kBatchMaxGroups):
+//   * slots are assigned through a per-warp permutation: the next tile's group j takes the slot the
+//     back substitution freed (B-1-j)-th, and groups beyond B take the slots this tile left unused;
+//   * full and empty barriers belong to slots (a phase bit per slot), not to groups.
+// E of the warp's current item is staged in a per-warp shared buffer when the item changes.
+constexpr int kBatchMaxGroups = 8;  // lines up to 256 voxels
+constexpr int kBatchWarps = 4;
+
+struct alignas(64) BatchItem {
+    CUtensorMap tm[3];
+    SubDev sd;
+    Geom g;
+    long long tile0[3];  // first tile of this item in each axis' list
+    int B, exact;
+};
+struct SrcItem {
+    float* p;
+    const float* rate;
+    const int* list;
+    const int* count;
+    float b, dt;
+    int N, P;
+};
+struct BatchArgs {
+    const BatchItem* items;
+    int nitems;
+    long long total[3];
+    int* err;
+};
+
+__device__ __forceinline__ uint32_t perm_get(uint32_t perm, int g) { return (perm >> (4 * g)) & 15u; }
+// next tile's permutation: the first B entries reversed, the rest kept
+__device__ __forceinline__ uint32_t perm_next(uint32_t perm, int B) {
+    uint32_t out = perm;
+    for (int j = 0; j < B; ++j) {
+        out &= ~(15u << (4 * j));
+        out |= perm_get(perm, B - 1 - j) << (4 * j);
+    }
+    return out;
+}
+__device__ __forceinline__ uint32_t perm_identity() {
+    uint32_t p = 0;
+    for (int j = 0; j < 8; ++j) p |= (uint32_t)j << (4 * j);
+    return p;
+}
+
+struct BTile {
+    int item;
+    int c0, c2;
+    bool interior_lane, flagged_lane;
+};
+
+// Item and TMA coordinates of tile t; `item` is a cursor that only moves forward (tiles of a warp
+// increase), so the search is a short scan.
+template <int AXIS>
+__device__ __forceinline__ BTile btile(const BatchArgs& a, long long t, int& item) {
+    while (item + 1 < a.nitems && t >= a.items[item + 1].tile0[AXIS]) ++item;
+    const BatchItem& it = a.items[item];
+    const int N = it.g.N, P = it.g.P;
+    const long long tt = t - it.tile0[AXIS];
+    BTile d;
+    d.item = item;
+    d.c2 = 0;
+    d.interior_lane = d.flagged_lane = false;
+    if (AXIS == 0) {
+        d.c0 = (int)(tt * 32);
+        const long long line = (long long)d.c0 + (threadIdx.x & 31);
+        const bool valid = line < (long long)N * N;
+        const int y = valid ? (int)(line % N) : 0, z = valid ? (int)(line / N) : 0;
+        d.interior_lane = valid && y >= 2 && y < N - 2 && z >= 2 && z < N - 2;
+        d.flagged_lane = valid && it.sd.line_flag[line] != 0u;
+    } else if (AXIS == 1) {
+        const int ntx = (P + 31) / 32;
+        d.c2 = (int)(tt / ntx);
+        d.c0 = (int)(tt - (long long)d.c2 * ntx) * 32;
+    } else {
+        d.c0 = (int)(tt * 32);
+    }
+    return d;
+}
+
+template <int AXIS>
+__device__ __forceinline__ void bbox_load(const BatchItem& it, const BTile& d, int g, float* slot, uint64_t* bar) {
+    mbar_arrive_expect(bar, kSlotFloats * 4);
+    if (AXIS == 0) tma_load_2d(slot, &it.tm[0], 32 * g, d.c0, bar);
+    else if (AXIS == 1) tma_load_3d(slot, &it.tm[1], d.c0, 32 * g, d.c2, bar);
+    else tma_load_2d(slot, &it.tm[2], d.c0, 32 * g, bar);
+}
+template <int AXIS>
+__device__ __forceinline__ void bbox_store(const BatchItem& it, const BTile& d, int g, const float* slot) {
+    if (AXIS == 0) tma_store_2d(&it.tm[0], 32 * g, d.c0, slot);
+    else if (AXIS == 1) tma_store_3d(&it.tm[1], d.c0, 32 * g, d.c2, slot);
+    else tma_store_2d(&it.tm[2], d.c0, 32 * g, slot);
+}
+
+template <int AXIS>
+__device__ __forceinline__ bool batch_tile(const BatchArgs& a, const BatchItem& it, const BTile& d, float* buf,
+                                           uint64_t* full, uint64_t* empty, const float* sE, uint32_t perm,
+                                           uint32_t& fph) {
+    const int N = it.g.N;
+    const int B = it.B;
+    const int lane = threadIdx.x & 31;
+    const SubDev& sd = it.sd;
+    SweepCtx c;
+    c.E = sE;
+    c.FR = sd.FRS;
+    c.b = sd.b;
+    c.dt = 0.f;
+    uint32_t special = 0;
+    XReset xr{0, 0, c.b};
+    if (AXIS == 0) {
+        const bool sp = !d.flagged_lane && !d.interior_lane;
+        xr.lo = d.flagged_lane ? 1 : (d.interior_lane ? 2 : 0x7fffffff);
+        xr.hi = d.flagged_lane ? N - 2 : N - 3;
+        special = __ballot_sync(FULL, sp);
+    }
+    float Y = c.b;
+    for (int g = 0; g < B; ++g) {
+        const int s = (int)perm_get(perm, g);
+        if (!mbar_wait(full + s, (fph >> s) & 1u, a.err, 1 + AXIS)) return false;
+        fph ^= 1u << s;
+        float* slot = buf + (size_t)s * kSlotFloats;
+        const bool edge = g == 0 || 32 * g + 31 > N - 3;
+        const bool rs = AXIS == 0 && (edge || special != 0);
+        if (AXIS != 0 && edge) edge_rows<AXIS>(c, slot, g, N, lane);
+        if ((sd.uni >> g) & 1u) forward_uniform<AXIS>(slot, g, lane, Y, sd.nE, rs, xr);
+        else forward_group<AXIS>(c, slot, g, lane, Y, rs, xr);
+    }
+    float x = c.b;
+    for (int g = B - 1; g >= 0; --g) {
+        const int s = (int)perm_get(perm, g);
+        float* slot = buf + (size_t)s * kSlotFloats;
+        backward_group<AXIS>(c, sd, slot, g, lane, x, it.exact);
+        fence_proxy_async();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(empty + s);
+    }
+    return true;
+}
+
+template <int AXIS>
+__device__ void batch_producer(const BatchArgs& a, float* buf, uint64_t* full, uint64_t* empty, long long t,
+                               long long step) {
+    const long long total = a.total[AXIS];
+    int item = 0;
+    BTile d = btile<AXIS>(a, t, item);
+    uint32_t perm = perm_identity(), eph = 0;
+    {
+        const BatchItem& it = a.items[d.item];
+        for (int g = 0; g < it.B; ++g) bbox_load<AXIS>(it, d, g, buf + (size_t)g * kSlotFloats, full + g);
+    }
+    for (;;) {
+        const BatchItem& it = a.items[d.item];
+        const int B = it.B;
+        const long long tn = t + step;
+        const bool has_next = tn < total;
+        int itemn = item;
+        const BTile dn = has_next ? btile<AXIS>(a, tn, itemn) : d;
+        const BatchItem& itn = a.items[dn.item];
+        const int Bn = has_next ? itn.B : 0;
+        for (int g = B - 1; g >= 0; --g) {
+            const int s = (int)perm_get(perm, g);
+            if (!mbar_wait1(empty + s, (eph >> s) & 1u, a.err, 8 + AXIS)) {
+                asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+                return;
+            }
+            eph ^= 1u << s;
+            bbox_store<AXIS>(it, d, g, buf + (size_t)s * kSlotFloats);
+            bulk_commit();
+            if (has_next && g + 1 <= B - 1 && B - 2 - g < Bn) {
+                // the store of group g+1 has read its slot: it takes the next tile's group B-2-g
+                bulk_wait_read<1>();
+                const int s1 = (int)perm_get(perm, g + 1);
+                bbox_load<AXIS>(itn, dn, B - 2 - g, buf + (size_t)s1 * kSlotFloats, full + s1);
+            }
+        }
+        if (!has_next) break;
+        bulk_wait_read<0>();
+        if (B - 1 < Bn) {
+            const int s0 = (int)perm_get(perm, 0);
+            bbox_load<AXIS>(itn, dn, B - 1, buf + (size_t)s0 * kSlotFloats, full + s0);
+        }
+        for (int j = B; j < Bn; ++j) {  // slots this tile left unused
+            const int sj = (int)perm_get(perm, j);
+            bbox_load<AXIS>(itn, dn, j, buf + (size_t)sj * kSlotFloats, full + sj);
+        }
+        perm = perm_next(perm, B);
+        t = tn;
+        d = dn;
+        item = itemn;
+    }
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
+// blockDim = 2W warps: W compute warps, then their W producer warps.  Shared memory: W x Bmax slots,
+// per-warp E buffers of Namax floats, then the slot barriers.
+template <int AXIS>
+__global__ void __launch_bounds__(64 * kBatchWarps, 1) k_sweep_batch(const __grid_constant__ BatchArgs a, int Bmax) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    const int W = blockDim.x >> 6, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int Namax = 32 * Bmax;
+    const uint32_t base = smem_u32(sm);
+    unsigned char* sm1 = sm + ((1024 - (base & 1023)) & 1023);
+    float* slots = reinterpret_cast<float*>(sm1);
+    float* sEs = reinterpret_cast<float*>(sm1 + (size_t)W * Bmax * kSlotFloats * 4);
+    uint64_t* full = reinterpret_cast<uint64_t*>(sm1 + (size_t)W * Bmax * kSlotFloats * 4 + align128(W * Namax * 4));
+    uint64_t* empty = full + W * kBatchMaxGroups;
+    for (int i = threadIdx.x; i < W * kBatchMaxGroups; i += blockDim.x) {
+        mbar_init(full + i, 1u);
+        mbar_init(empty + i, 1u);
+    }
+    fence_mbar_init();
+    __syncthreads();
+    const long long total = a.total[AXIS];
+    const long long step = (long long)gridDim.x * W;
+    if (warp >= W) {
+        const int w = warp - W;
+        const long long t = (long long)blockIdx.x * W + w;
+        if (lane == 0 && t < total)
+            batch_producer<AXIS>(a, slots + (size_t)w * Bmax * kSlotFloats, full + w * kBatchMaxGroups,
+                                 empty + w * kBatchMaxGroups, t, step);
+        return;
+    }
+    float* buf = slots + (size_t)warp * Bmax * kSlotFloats;
+    float* sE = sEs + (size_t)warp * Namax;
+    uint64_t* fb = full + warp * kBatchMaxGroups;
+    uint64_t* eb = empty + warp * kBatchMaxGroups;
+    uint32_t perm = perm_identity(), fph = 0;
+    int item = 0, staged = -1;
+    for (long long t = (long long)blockIdx.x * W + warp; t < total; t += step) {
+        const BTile d = btile<AXIS>(a, t, item);
+        const BatchItem& it = a.items[d.item];
+        if (d.item != staged) {
+            // E of the elements the reference's recurrences update; 0 elsewhere (identity)
+            const int N = it.g.N;
+            __syncwarp();
+            for (int j = lane; j < 32 * it.B; j += 32) sE[j] = (j >= 1 && j <= N - 2) ? it.sd.EFR[j] : 0.f;
+            __syncwarp();
+            staged = d.item;
+        }
+        if (!batch_tile<AXIS>(a, it, d, buf, fb, eb, sE, perm, fph)) break;
+        perm = perm_next(perm, it.B);
+    }
+}
+
+// Setboundary + meshupdatekernel on the listed uptake lines of every item (k_source_lines over
+// many grids).
+__global__ void k_source_lines_batch(const SrcItem* items, int nitems) {
+    const int lane = threadIdx.x & 31;
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (int s = 0; s < nitems; ++s) {
+        const SrcItem& it = items[s];
+        const int N = it.N;
+        const int cnt = *it.count;
+        for (long long li = gw; li < cnt; li += nw) {
+            const int line = it.list[li];
+            const int y = line % N, z = line / N;
+            const bool bl = y < 2 || y >= N - 2 || z < 2 || z >= N - 2;
+            float* pl = it.p + (long long)line * it.P;
+            const float* rl = it.rate + (long long)line * it.P;
+            for (int j = lane; j < N; j += 32) {
+                const float v = (bl || j < 2 || j > N - 3) ? it.b : pl[j];
+                pl[j] = __fdiv_rn(v, __fmaf_rn(-rl[j], it.dt, 1.f));
+            }
+        }
+    }
+}
+
 // The bounded wait's give-up path: nothing ever arrives on this barrier, so the wait must stop after
 // `polls` polls and record code 12 in the context's error word, as a sweep does when a box never
 // lands.  Run by gell_selftest_timeout; the context stays usable afterwards.
@@ -1088,6 +1366,105 @@ gell_status lod_solver(gell_ctx* c, int sub, int substeps) {
         GELL_KERNEL(c, "k_sweep_x", k_sweep<0><<<gx, w * 64, smem, c->stream>>>(ax));
         GELL_KERNEL(c, "k_sweep_y", k_sweep<1><<<gy, w * 64, smem, c->stream>>>(ay));
         GELL_KERNEL(c, "k_sweep_z", k_sweep<2><<<gz, w * 64, smem, c->stream>>>(az));
+    }
+    return GELL_OK;
+}
+
+// ------------------------------------------------------------------ batched sweeps: host side
+
+struct LodBatch {
+    BatchItem* d_items = nullptr;
+    SrcItem* d_src = nullptr;
+    int nitems = 0;
+    long long total[3] = {0, 0, 0};
+    int Bmax = 0;
+    gell_ctx* c0 = nullptr;  // launches counted and timeouts reported on the first member
+};
+
+gell_status lod_batch_build(const std::vector<gell_ctx*>& ms, LodBatch** out) {
+    *out = nullptr;
+    std::vector<BatchItem> items;
+    std::vector<SrcItem> src;
+    long long tot[3] = {0, 0, 0};
+    int Bmax = 0;
+    for (gell_ctx* c : ms) {
+        const int N = c->g.N, P = c->g.P;
+        const int B = (N + 31) / 32;
+        if (B > kBatchMaxGroups) return GELL_ERR_UNSUPPORTED;
+        for (Substrate& S : c->subs) {
+            BatchItem it;
+            std::memset(&it, 0, sizeof(it));
+            for (int k = 0; k < 3; ++k) it.tm[k] = S.tmap[k];
+            const float R = S.conv_R;
+            it.sd = SubDev{S.p,    S.rate,           S.line_flag, S.EF,        S.FRS,      S.s.boundary, S.side,
+                           S.uniform_groups, -S.E[N - 2], -S.side, -(S.side * R), -S.F[N - 2], R};
+            it.g = c->g;
+            it.B = B;
+            it.exact = c->exact_chain ? 1 : 0;
+            const long long tiles[3] = {((long long)N * N + 31) / 32, (long long)((P + 31) / 32) * N,
+                                        (c->g.PN + 31) / 32};
+            for (int k = 0; k < 3; ++k) {
+                it.tile0[k] = tot[k];
+                tot[k] += tiles[k];
+            }
+            items.push_back(it);
+            src.push_back(SrcItem{S.p, S.rate, S.line_list, S.line_count, S.s.boundary, c->P.diffusion_dt, N, P});
+            if (B > Bmax) Bmax = B;
+        }
+    }
+    if (items.empty()) return GELL_ERR_INVALID_ARG;
+    LodBatch* b = new LodBatch;
+    b->nitems = (int)items.size();
+    for (int k = 0; k < 3; ++k) b->total[k] = tot[k];
+    b->Bmax = Bmax;
+    b->c0 = ms[0];
+    bool ok = cudaMalloc((void**)&b->d_items, sizeof(BatchItem) * items.size()) == cudaSuccess &&
+              cudaMalloc((void**)&b->d_src, sizeof(SrcItem) * src.size()) == cudaSuccess &&
+              cudaMemcpy(b->d_items, items.data(), sizeof(BatchItem) * items.size(), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(b->d_src, src.data(), sizeof(SrcItem) * src.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+    static bool configured[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (ok && dev >= 0 && dev < 64 && !configured[dev]) {
+        for (const void* k : {(const void*)k_sweep_batch<0>, (const void*)k_sweep_batch<1>, (const void*)k_sweep_batch<2>})
+            ok = ok && cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) == cudaSuccess;
+        configured[dev] = ok;
+    }
+    if (!ok) {
+        cudaGetLastError();
+        lod_batch_free(b);
+        return GELL_ERR_CUDA;
+    }
+    *out = b;
+    return GELL_OK;
+}
+
+void lod_batch_free(LodBatch* b) {
+    if (!b) return;
+    if (b->d_items) cudaFree(b->d_items);
+    if (b->d_src) cudaFree(b->d_src);
+    delete b;
+}
+
+gell_status lod_batch_run(LodBatch* b, cudaStream_t st, int substeps) {
+    gell_ctx* c = b->c0;
+    const int W = kBatchWarps;
+    const int Namax = 32 * b->Bmax;
+    const int smem = 1024 + W * b->Bmax * kSlotFloats * 4 + align128(W * Namax * 4) + 2 * W * kBatchMaxGroups * 8;
+    BatchArgs a{};
+    a.items = b->d_items;
+    a.nitems = b->nitems;
+    for (int k = 0; k < 3; ++k) a.total[k] = b->total[k];
+    a.err = c->dev_err;
+    auto grid = [&](long long tiles) {
+        const long long want = (tiles + W - 1) / W;
+        return (int)(want < num_sms() ? want : num_sms());
+    };
+    for (int k = 0; k < substeps; ++k) {
+        GELL_KERNEL(c, "k_source_lines", k_source_lines_batch<<<num_sms() * 8, 256, 0, st>>>(b->d_src, b->nitems));
+        GELL_KERNEL(c, "k_sweep_x", k_sweep_batch<0><<<grid(a.total[0]), W * 64, smem, st>>>(a, b->Bmax));
+        GELL_KERNEL(c, "k_sweep_y", k_sweep_batch<1><<<grid(a.total[1]), W * 64, smem, st>>>(a, b->Bmax));
+        GELL_KERNEL(c, "k_sweep_z", k_sweep_batch<2><<<grid(a.total[2]), W * 64, smem, st>>>(a, b->Bmax));
     }
     return GELL_OK;
 }

@@ -348,9 +348,14 @@ gell_status gell_reference_spheroid(const gell_params* p, int n, float cell_radi
  * biology steps and transfers stay per member (gell_cell_birth / gell_cell_death, ...).
  * gell_ensemble_configure sets the branch count (1..64) and the sweeps' line tiles per CTA
  * (GELL_OPT_SWEEP_WARPS, 0..4) of every member.  gell_ensemble_tune times branch counts 1, 2, 4, ..
- * and tile widths 0, 2, 1 with real steps of the members (2 per trial, plus one first step; the
- * total is returned in *steps_taken) and keeps the fastest.  The members must outlive the ensemble
- * and live on the device that is current when it is created.
+ * and tile widths 0, 2, 1, then the batched LOD, with real steps of the members (2 per trial, plus
+ * one first step; the total is returned in *steps_taken) and keeps the fastest.  The members must
+ * outlive the ensemble and live on the device that is current when it is created.
+ * gell_ensemble_set_batched (0 or 1, default 0): every captured step runs the members' FM_update and
+ * PreLOD on the branches, then the LOD substeps of ALL members as one launch per sweep axis (and one
+ * for the uptake source) over a device-side list of every member's line tiles; grid edges up to 256.
+ * Results are identical either way.  gell_ensemble_get_batched reports the setting (after a tune,
+ * whether the tuner chose it).
  */
 typedef struct gell_ensemble gell_ensemble;
 gell_status gell_ensemble_create(gell_ctx* const* members, int count, gell_ensemble** out);
@@ -360,6 +365,8 @@ gell_status gell_ensemble_run_mechanics(gell_ensemble* ens, int steps, int subst
 gell_status gell_ensemble_tune(gell_ensemble* ens, int substeps, int* steps_taken, int* best_branches,
                                int* best_sweep_warps);
 gell_status gell_ensemble_sync(gell_ensemble* ens);
+gell_status gell_ensemble_set_batched(gell_ensemble* ens, int on);
+gell_status gell_ensemble_get_batched(const gell_ensemble* ens, int* on);
 
 /* Learned surrogate of one substrate's LOD (no reference counterpart; the reference's plain solver,
  * LODsolver in include/LODkernel.cuh:280-300, is its fallback and the source of its training pairs).

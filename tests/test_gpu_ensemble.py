@@ -81,3 +81,43 @@ def test_ensemble_across_birth_and_death_and_tuning():
             np.testing.assert_array_equal(x, y)
     for m in alone + together:
         m.close()
+
+
+def test_batched_lod_matches_members_stepped_alone():
+    """gell_ensemble_set_batched: the LOD substeps of all members as one launch per sweep over a
+    work list of every member's line tiles.  Members of 1 to 7 groups per line (N = 32 .. 200), one
+    with two substrates, so consecutive tiles of a warp differ in length; across birth and death."""
+    sizes = [(32, 1500), (48, 800), (100, 6000), (131, 9000), (200, 20000), (64, 2500)]
+
+    def make():
+        ms = [member(i, N, n) for i, (N, n) in enumerate(sizes)]
+        ms[2].add_substrate(gb.drug())
+        return ms
+
+    alone, together = make(), make()
+    with gb.Ensemble(together) as ens:
+        ens.configure(branches=4, sweep_warps=0)
+        ens.set_batched(True)
+        assert ens.batched()
+        for a in alone:
+            for _ in range(5):
+                a.mechanics_step(4)
+        ens.run_mechanics(5, 4)
+        for a, b in zip(alone, together):
+            a.CellBirth_kernel()
+            b.CellBirth_kernel()
+        for a in alone:
+            for _ in range(4):
+                a.mechanics_step(4)
+        ens.run_mechanics(4, 4)
+        for a, b in zip(alone, together):
+            a.CellDeath_kernel()
+            b.CellDeath_kernel()
+        ens.sync()
+    for a, b in zip(alone, together):
+        assert a.count() == b.count()
+        np.testing.assert_array_equal(raw(a.export_cells()), raw(b.export_cells()))
+        np.testing.assert_array_equal(a.field(0).view(np.uint32), b.field(0).view(np.uint32))
+    np.testing.assert_array_equal(alone[2].field(1).view(np.uint32), together[2].field(1).view(np.uint32))
+    for m in alone + together:
+        m.close()
