@@ -408,7 +408,8 @@ def run_c3(args, rank, world, local_rank):
 C4_MEMBERS, C4_BIO = 64, 60
 C4_WORKLOAD = ("batched ensemble: 64 independent instances, grid edge log-uniform in [64, 200] voxels of 10 um, "
                "cells log-uniform in [2,000, 200,000], D U(5e4, 2e5), uptake U(5, 20)/min (seed 7), one FP32 "
-               "substrate each, Philox birth/death; one graph of parallel branches, tuned")
+               "substrate each, Philox birth/death; one graph of parallel branches (LOD per member or batched "
+               "over all members), tuned")
 
 
 def c4_members(gb, stream):
@@ -569,6 +570,7 @@ def run_c4(args, rank, world, local_rank):
     sims, edges = c4_members(gb, stream)
     ens = gb.Ensemble(sims)
     taken, branches, warps = ens.tune(SUBSTEPS)
+    batched = ens.batched()
     ens.run_mechanics(max(0, args.warmup - taken) + 2, SUBSTEPS)
     ens.sync()
     ncells0 = sum(s.count() for s in sims)
@@ -626,6 +628,7 @@ def run_c4(args, rank, world, local_rank):
             "config": {"workload": C4_WORKLOAD, "members": C4_MEMBERS, "voxels_total": int((edges ** 3).sum()),
                        "cells_total_start": int(ncells0), "substeps_per_step": SUBSTEPS,
                        "biology_period_steps": C4_BIO, "tuned_branches": branches, "tuned_sweep_warps": warps,
+                       "tuned_batched_lod": batched,
                        "tuning_steps": taken, "parallelism": "replicas"},
             "components": {"ms_per_step_members_one_by_one": t_seq_step,
                            "speedup_vs_members_one_by_one": t_seq_step / (times[0] / K)},
