@@ -767,8 +767,10 @@ __global__ void __launch_bounds__(32 * kRingWarps, 1) k_sweep_ring(const __grid_
 // One launch per axis sweeps the lines of MANY grids: every (member, substrate) pair of an
 // ensemble is an item with its own geometry, tensor maps and Thomas tables, and the items' line
 // tiles form one list that the persistent CTAs walk (warp w of CTA b takes tiles b*W + w + k*step).
-// The line-tile pipeline is the one above (a producer lane per compute warp, whole tiles in
-// shared memory), with two changes for tiles of different lengths (B groups, up to kBatchMaxGroups):
+// Each warp takes a contiguous range of the list holding an equal share of the work (a tile of B
+// groups costs B + 1), so it stays on one item for many tiles.  The line-tile pipeline is the one
+// above (a producer lane per compute warp, whole tiles in shared memory), with two changes for tiles
+// of different lengths (B groups, up to kBatchMaxGroups):
 //   * slots are assigned through a per-warp permutation: the next tile's group j takes the slot the
 //     back substitution freed (B-1-j)-th, and groups beyond B take the slots this tile left unused;
 //   * full and empty barriers belong to slots (a phase bit per slot), not to groups.
@@ -781,6 +783,7 @@ struct alignas(64) BatchItem {
     SubDev sd;
     Geom g;
     long long tile0[3];  // first tile of this item in each axis' list
+    long long cost0[3];  // work of the items before it (a tile costs B + 1)
     int B, exact;
 };
 struct SrcItem {
@@ -795,8 +798,23 @@ struct BatchArgs {
     const BatchItem* items;
     int nitems;
     long long total[3];
+    long long cost[3];  // total work per axis
     int* err;
 };
+
+// First tile whose work starts at or after `x`: the warps split the tiles into contiguous ranges
+// of equal work (tiles of long lines cost more), so a warp stays on one item for many tiles.
+template <int AXIS>
+__device__ __forceinline__ long long tile_at_cost(const BatchArgs& a, long long x) {
+    if (x >= a.cost[AXIS]) return a.total[AXIS];
+    int i = 0;
+    while (i + 1 < a.nitems && a.items[i + 1].cost0[AXIS] <= x) ++i;
+    const BatchItem& it = a.items[i];
+    const long long c = it.B + 1;
+    long long j = it.tile0[AXIS] + (x - it.cost0[AXIS] + c - 1) / c;
+    const long long end = i + 1 < a.nitems ? a.items[i + 1].tile0[AXIS] : a.total[AXIS];
+    return j < end ? j : end;
+}
 
 __device__ __forceinline__ uint32_t perm_get(uint32_t perm, int g) { return (perm >> (4 * g)) & 15u; }
 // next tile's permutation: the first B entries reversed, the rest kept
@@ -910,8 +928,9 @@ __device__ __forceinline__ bool batch_tile(const BatchArgs& a, const BatchItem& 
 
 template <int AXIS>
 __device__ void batch_producer(const BatchArgs& a, float* buf, uint64_t* full, uint64_t* empty, long long t,
-                               long long step) {
-    const long long total = a.total[AXIS];
+                               long long t_end) {
+    const long long step = 1;
+    const long long total = t_end;
     int item = 0;
     BTile d = btile<AXIS>(a, t, item);
     uint32_t perm = perm_identity(), eph = 0;
@@ -981,14 +1000,15 @@ __global__ void __launch_bounds__(64 * kBatchWarps, 1) k_sweep_batch(const __gri
     }
     fence_mbar_init();
     __syncthreads();
-    const long long total = a.total[AXIS];
-    const long long step = (long long)gridDim.x * W;
+    // this warp pair's contiguous range of tiles: an equal share of the axis' work
+    const int wi = warp >= W ? warp - W : warp;
+    const long long nwg = (long long)gridDim.x * W, wg = (long long)blockIdx.x * W + wi;
+    const long long t_begin = tile_at_cost<AXIS>(a, a.cost[AXIS] * wg / nwg);
+    const long long t_end = tile_at_cost<AXIS>(a, a.cost[AXIS] * (wg + 1) / nwg);
     if (warp >= W) {
-        const int w = warp - W;
-        const long long t = (long long)blockIdx.x * W + w;
-        if (lane == 0 && t < total)
-            batch_producer<AXIS>(a, slots + (size_t)w * Bmax * kSlotFloats, full + w * kBatchMaxGroups,
-                                 empty + w * kBatchMaxGroups, t, step);
+        if (lane == 0 && t_begin < t_end)
+            batch_producer<AXIS>(a, slots + (size_t)wi * Bmax * kSlotFloats, full + wi * kBatchMaxGroups,
+                                 empty + wi * kBatchMaxGroups, t_begin, t_end);
         return;
     }
     float* buf = slots + (size_t)warp * Bmax * kSlotFloats;
@@ -997,7 +1017,7 @@ __global__ void __launch_bounds__(64 * kBatchWarps, 1) k_sweep_batch(const __gri
     uint64_t* eb = empty + warp * kBatchMaxGroups;
     uint32_t perm = perm_identity(), fph = 0;
     int item = 0, staged = -1;
-    for (long long t = (long long)blockIdx.x * W + warp; t < total; t += step) {
+    for (long long t = t_begin; t < t_end; ++t) {
         const BTile d = btile<AXIS>(a, t, item);
         const BatchItem& it = a.items[d.item];
         if (d.item != staged) {
@@ -1376,7 +1396,7 @@ struct LodBatch {
     BatchItem* d_items = nullptr;
     SrcItem* d_src = nullptr;
     int nitems = 0;
-    long long total[3] = {0, 0, 0};
+    long long total[3] = {0, 0, 0}, cost[3] = {0, 0, 0};
     int Bmax = 0;
     gell_ctx* c0 = nullptr;  // launches counted and timeouts reported on the first member
 };
@@ -1385,7 +1405,7 @@ gell_status lod_batch_build(const std::vector<gell_ctx*>& ms, LodBatch** out) {
     *out = nullptr;
     std::vector<BatchItem> items;
     std::vector<SrcItem> src;
-    long long tot[3] = {0, 0, 0};
+    long long tot[3] = {0, 0, 0}, cost[3] = {0, 0, 0};
     int Bmax = 0;
     for (gell_ctx* c : ms) {
         const int N = c->g.N, P = c->g.P;
@@ -1405,7 +1425,9 @@ gell_status lod_batch_build(const std::vector<gell_ctx*>& ms, LodBatch** out) {
                                         (c->g.PN + 31) / 32};
             for (int k = 0; k < 3; ++k) {
                 it.tile0[k] = tot[k];
+                it.cost0[k] = cost[k];
                 tot[k] += tiles[k];
+                cost[k] += tiles[k] * (B + 1);
             }
             items.push_back(it);
             src.push_back(SrcItem{S.p, S.rate, S.line_list, S.line_count, S.s.boundary, c->P.diffusion_dt, N, P});
@@ -1415,7 +1437,10 @@ gell_status lod_batch_build(const std::vector<gell_ctx*>& ms, LodBatch** out) {
     if (items.empty()) return GELL_ERR_INVALID_ARG;
     LodBatch* b = new LodBatch;
     b->nitems = (int)items.size();
-    for (int k = 0; k < 3; ++k) b->total[k] = tot[k];
+    for (int k = 0; k < 3; ++k) {
+        b->total[k] = tot[k];
+        b->cost[k] = cost[k];
+    }
     b->Bmax = Bmax;
     b->c0 = ms[0];
     bool ok = cudaMalloc((void**)&b->d_items, sizeof(BatchItem) * items.size()) == cudaSuccess &&
@@ -1454,7 +1479,10 @@ gell_status lod_batch_run(LodBatch* b, cudaStream_t st, int substeps) {
     BatchArgs a{};
     a.items = b->d_items;
     a.nitems = b->nitems;
-    for (int k = 0; k < 3; ++k) a.total[k] = b->total[k];
+    for (int k = 0; k < 3; ++k) {
+        a.total[k] = b->total[k];
+        a.cost[k] = b->cost[k];
+    }
     a.err = c->dev_err;
     auto grid = [&](long long tiles) {
         const long long want = (tiles + W - 1) / W;
