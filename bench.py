@@ -629,6 +629,8 @@ def run_c4(args, rank, world, local_rank):
                        "cells_total_start": int(ncells0), "substeps_per_step": SUBSTEPS,
                        "biology_period_steps": C4_BIO, "tuned_branches": branches, "tuned_sweep_warps": warps,
                        "tuned_batched_lod": batched,
+                       "cells_cap": "each member's draw capped at 0.35 of its domain volume at packing 0.6, so the "
+                                    "spheroid (radius 0.44 of the edge) fits its grid",
                        "tuning_steps": taken, "parallelism": "replicas"},
             "components": {"ms_per_step_members_one_by_one": t_seq_step,
                            "speedup_vs_members_one_by_one": t_seq_step / (times[0] / K)},

@@ -43,3 +43,38 @@ def test_five_mechanics_steps_match_the_reference_build():
         same = np.mean(gf.view(np.uint32) == ef.view(np.uint32))
         print(f"field voxels bit-identical with the reference build after {steps} steps: {same:.6f}")
         np.testing.assert_allclose(gf, ef, rtol=1e-5, atol=0)
+
+
+@pytest.mark.skipif(not (ref_lib.available("c2") and ref_lib.available("c2d")),
+                    reason="reference build oracle/_ref missing")
+def test_large_workload_whole_steps_match_the_reference_build():
+    """The large plain-method workload (400^3, oxygen + drug, the bench's 10^6-cell lattice
+    spheroid), three whole steps (FM_update, PreLOD of both substrates, 10 LODsolver substeps of
+    both) through the reference's facades and through gell_b200's graph-driven step loop: cells bit
+    for bit, both fields within 1e-5 relative (float-atomic uptake sums, as in the reference)."""
+    N, length, steps = 400, 10.0, 3
+    cells = gb.lattice_spheroid(1_000_000, N * length / 2, 0, length, N)
+    with ref_lib.RefSim("c2", 38.0, 1e5, 0.1) as o2, ref_lib.RefSim("c2d", 1.0, 5e4, 0.05) as drug, \
+            gb.Simulation(voxel_num=N, voxel_length=length, max_cell_num=o2.cap) as sim:
+        o2.set_cells(cells)
+        sim.add_substrate(gb.oxygen())
+        sim.add_substrate(gb.drug())
+        sim.import_cells(cells)
+        for _ in range(steps):
+            o2.fm_update()
+            o2.prelod()
+            drug.prelod_on(o2)
+            o2.lodsolver(10)
+            drug.lodsolver(10)
+        sim.run_mechanics(steps, 10)
+        got, exp = sim.export_cells(), o2.cells()
+        assert len(got) == len(exp)
+        for f in ("sign", "mesh_idx", "phase"):
+            np.testing.assert_array_equal(got[f], exp[f], err_msg=f)
+        for f in ("pos", "oldforce", "r", "V"):
+            np.testing.assert_array_equal(got[f].view(np.uint32), exp[f].view(np.uint32), err_msg=f)
+        for sub, ref in ((0, o2), (1, drug)):
+            gf, ef = sim.field(sub), ref.field()
+            same = np.mean(gf.view(np.uint32) == ef.view(np.uint32))
+            print(f"substrate {sub}: voxels bit-identical with the reference build after {steps} steps: {same:.6f}")
+            np.testing.assert_allclose(gf, ef, rtol=1e-5, atol=0)
