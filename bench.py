@@ -475,7 +475,7 @@ def run_c5(args, rank, world, local_rank):
     sim.PreLOD()
     sim.LODsolver(C5_WARM, 0)  # from the boundary value to a quasi-steady field
     sim.set_conv_ring(not args.no_conv_ring)
-    sim.surrogate_load(0, sw.weights, K, sw.rate_scale, sw.threshold)
+    sim.surrogate_load(0, sw.weights, K, sw.rate_scale, sw.threshold, sw.input_kind)
     b = float(gb.oxygen().boundary)
     inner = ~gs.shell_mask(C5_N)
     for _ in range(args.warmup):  # untimed: kernels loaded, buffers touched

@@ -415,8 +415,10 @@ class Simulation:
 
     # -- learned surrogate of one substrate's LOD
     def surrogate_load(self, sub: int, weights: np.ndarray, substeps: int = 50, rate_scale: float = 0.1,
-                       threshold: float = 1e-3) -> None:
-        """Load the operator's weights (gell_surrogate_weight_count() floats, conv3d order)."""
+                       threshold: float = 1e-3, input_kind: int = 0) -> None:
+        """Load the operator's weights (gell_surrogate_weight_count() floats, conv3d order); input_kind
+        is the form the weights were trained for (GELL_OPT_SURROGATE_INPUT: 0 field, 1 one-substep change)."""
+        self._check(self.lib.gell_set_option(self.h, 9, int(input_kind)), "gell_set_option")
         w = np.ascontiguousarray(weights, np.float32).reshape(-1)
         self._check(self.lib.gell_surrogate_load(self.h, sub, P(w.ctypes.data), w.size, substeps, rate_scale,
                                                  threshold), "gell_surrogate_load")
@@ -451,7 +453,9 @@ class Simulation:
         f = (raw.astype(np.uint32) << 16).view(np.float32).reshape(planes, n3, 8)
         return f.transpose(0, 2, 1).reshape(planes * 8, n3).copy()
 
-    def surrogate_train_init(self, sub: int, weights: np.ndarray, substeps: int = 50, rate_scale: float = 0.1) -> None:
+    def surrogate_train_init(self, sub: int, weights: np.ndarray, substeps: int = 50, rate_scale: float = 0.1,
+                             input_kind: int = 0) -> None:
+        self._check(self.lib.gell_set_option(self.h, 9, int(input_kind)), "gell_set_option")
         w = np.ascontiguousarray(weights, np.float32).reshape(-1)
         self._check(self.lib.gell_surrogate_train_init(self.h, sub, P(w.ctypes.data), w.size, substeps, rate_scale),
                     "gell_surrogate_train_init")

@@ -683,6 +683,10 @@ gell_status gell_set_option(gell_ctx* c, int option, int64_t value) {
             c->sweep_ring = (int)value;
             return GELL_OK;
         case GELL_OPT_SWEEP_L2HINT: c->sweep_l2hint = value != 0; return GELL_OK;
+        case GELL_OPT_SURROGATE_INPUT:
+            if (value < 0 || value > 1) return fail(c, GELL_ERR_INVALID_ARG, "surrogate input outside 0..1");
+            c->sur_input = (int)value;
+            return GELL_OK;
         case GELL_OPT_SWEEP_RING_LAG:
             if (value < 0 || value > 7) return fail(c, GELL_ERR_INVALID_ARG, "sweep ring lag outside 0..7");
             c->sweep_ring_lag = (int)value;

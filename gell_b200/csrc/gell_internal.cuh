@@ -115,6 +115,7 @@ struct gell_ctx {
     std::vector<gell::Substrate> subs;
     gell::SurrogateState* sur[8] = {};  // per substrate, created by gell_surrogate_load
     bool conv_ring = true;              // GELL_OPT_CONV_RING: the surrogate's convolutions reuse rows along y
+    int sur_input = 0;                  // GELL_OPT_SURROGATE_INPUT for surrogates loaded from now on
     bool rate_valid = false;
     bool exact_chain = false;  // GELL_OPT_EXACT_CHAIN
     int sweep_warps = 0;       // GELL_OPT_SWEEP_WARPS (0: as many as shared memory allows)

@@ -779,6 +779,25 @@ __global__ void k_pack_input(const float* p, const float* rate, Geom g, float in
     }
 }
 
+// Input planes of the delta form: channel 0 = (p1 - p0) / m (the change of one plain substep,
+// normalised by its largest magnitude inside the shell), channel 1 = rate * rate_scale, channel 2
+// = the shell mask.
+__global__ void k_pack_input_delta(const float* p1, const float* p0, const float* rate, Geom g, float inv_m,
+                                   float rate_scale, uint4* out) {
+    const long long nvox = (long long)g.N * g.N * g.N;
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < nvox;
+         v += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(v % g.N);
+        const long long yz = v / g.N;
+        const int y = (int)(yz % g.N), z = (int)(yz / g.N);
+        const long long pi = x + (long long)g.P * y + g.PN * z;
+        const int N = g.N;
+        const bool shell = x < 2 || x > N - 3 || y < 2 || y > N - 3 || z < 2 || z > N - 3;
+        const float d = shell ? 0.f : __fmul_rn(__fsub_rn(p1[pi], p0[pi]), inv_m);
+        out[v] = make_uint4(pack_bf16(d, __fmul_rn(rate[pi], rate_scale)), pack_bf16(shell ? 1.f : 0.f, 0.f), 0u, 0u);
+    }
+}
+
 // max |a - b| over the voxels inside the shell (the values the next substep carries forward), as
 // the bits of a non-negative float (ordered like the floats).
 __global__ void k_absdiff_max(const float* a, const float* b, Geom g, unsigned* out) {
@@ -925,6 +944,10 @@ struct TrainState {
 struct SurrogateState {
     int substeps = 0;
     float rate_scale = 0.f, threshold = 0.f;
+    // input channel 0: 0 = the field p / b; 1 = the change of one plain substep, (L(p) - p) / m with
+    // m = its largest magnitude inside the shell, and the output scaled by m instead of b
+    int input_kind = 0;
+    float* p0 = nullptr;        // field before the step (pitched), delta input
     uint8_t* w[kLayers] = {};   // packed weight images
     float* bias[kLayers] = {};  // padded to the layer's NOUT
     uint4* in = nullptr;        // 2 planes
@@ -945,7 +968,8 @@ void surrogate_free(gell_ctx* c) {
             if (s->w[l]) cudaFree(s->w[l]);
             if (s->bias[l]) cudaFree(s->bias[l]);
         }
-        for (void* p : {(void*)s->in, (void*)s->h, (void*)s->t, (void*)s->ph, (void*)s->backup, (void*)s->dmax})
+        for (void* p : {(void*)s->in, (void*)s->h, (void*)s->t, (void*)s->ph, (void*)s->backup, (void*)s->dmax,
+                        (void*)s->p0})
             if (p) cudaFree(p);
         if (s->hmax) cudaFreeHost(s->hmax);
         if (TrainState* t = s->train) {
@@ -1059,13 +1083,42 @@ static gell_status launch_conv(gell_ctx* c, const char* name, const CUtensorMap&
 //   layer 2k+1     t  = relu(conv_a(h))          (k = 0..3)
 //   layer 2k+2     h += conv_b(t)
 //   layer 9        S->ph = p + b * conv_out(h) inside the shell, b on it
+// The delta form's input planes: one plain substep from the field p0 (kept in S->p0), the largest
+// change m inside the shell (read back to the host), the planes packed from (L(p0) - p0) / m, and
+// the field put back to p0.  *m_out = m.
+static gell_status delta_input(gell_ctx* c, int sub, SurrogateState* S, float* m_out) {
+    Substrate& Su = c->subs[sub];
+    const size_t fb = (size_t)c->nvox_p * 4;
+    GELL_CUDA(c, cudaMemcpyAsync(S->p0, Su.p, fb, cudaMemcpyDeviceToDevice, c->stream));
+    gell_status st = lod_solver(c, sub, 1);
+    if (st != GELL_OK) return st;
+    GELL_CUDA(c, cudaMemsetAsync(S->dmax, 0, 4, c->stream));
+    GELL_KERNEL(c, "k_absdiff_max", (k_absdiff_max<<<148 * 8, 256, 0, c->stream>>>(Su.p, S->p0, c->g, S->dmax)));
+    GELL_CUDA(c, cudaMemcpyAsync(S->hmax, S->dmax, 4, cudaMemcpyDeviceToHost, c->stream));
+    GELL_CUDA(c, cudaStreamSynchronize(c->stream));
+    float m;
+    std::memcpy(&m, S->hmax, 4);
+    const int pb = blocks_for(c->nvox, 256);
+    GELL_KERNEL(c, "k_pack_input",
+                (k_pack_input_delta<<<pb < 148 * 16 ? pb : 148 * 16, 256, 0, c->stream>>>(
+                    Su.p, S->p0, Su.rate, c->g, m > 0.f ? 1.f / m : 0.f, S->rate_scale, S->in)));
+    GELL_CUDA(c, cudaMemcpyAsync(Su.p, S->p0, fb, cudaMemcpyDeviceToDevice, c->stream));
+    *m_out = m;
+    return GELL_OK;
+}
+
 static gell_status run_layers(gell_ctx* c, int sub, SurrogateState* S, int layers) {
     Substrate& Su = c->subs[sub];
     const float b = Su.s.boundary;
     const int pb = blocks_for(c->nvox, 256);
-    GELL_KERNEL(c, "k_pack_input",
-                (k_pack_input<<<pb < 148 * 16 ? pb : 148 * 16, 256, 0, c->stream>>>(Su.p, Su.rate, c->g, 1.f / b,
-                                                                                 S->rate_scale, S->in)));
+    float scale = b;  // the output's scale: b, or m in the delta form
+    if (S->input_kind == 1) {
+        if (gell_status sd = delta_input(c, sub, S, &scale)) return sd;
+    } else {
+        GELL_KERNEL(c, "k_pack_input",
+                    (k_pack_input<<<pb < 148 * 16 ? pb : 148 * 16, 256, 0, c->stream>>>(Su.p, Su.rate, c->g, 1.f / b,
+                                                                                     S->rate_scale, S->in)));
+    }
     gell_status st = GELL_OK;
     for (int l = 0; l < layers && st == GELL_OK; ++l) {
         const uint8_t* w = S->w[l];
@@ -1073,7 +1126,7 @@ static gell_status run_layers(gell_ctx* c, int sub, SurrogateState* S, int layer
         if (l == 0)
             st = launch_conv<2, 32, kRelu>(c, "k_conv3_in", S->map_in, w, bi, S->h, nullptr, nullptr, nullptr, nullptr, 0.f, 0.f);
         else if (l == kLayers - 1)
-            st = launch_conv<4, 16, kField>(c, "k_conv3_out", S->map_h, w, bi, nullptr, nullptr, nullptr, S->ph, Su.p, b, b);
+            st = launch_conv<4, 16, kField>(c, "k_conv3_out", S->map_h, w, bi, nullptr, nullptr, nullptr, S->ph, Su.p, scale, b);
         else if (l & 1)
             st = launch_conv<4, 32, kRelu>(c, "k_conv3_hidden", S->map_h, w, bi, S->t, nullptr, nullptr, nullptr, nullptr, 0.f, 0.f);
         else
@@ -1154,15 +1207,24 @@ static gell_status train_pair(gell_ctx* c, int sub, SurrogateState* S, float lr,
     const float b = Su.s.boundary;
     const size_t fb = (size_t)c->nvox_p * 4;
     GELL_CUDA(c, cudaMemcpyAsync(S->backup, Su.p, fb, cudaMemcpyDeviceToDevice, c->stream));
-    gell_status st = lod_solver(c, sub, S->substeps);
+    // delta form: the input planes from one plain substep first (the field is put back), the output
+    // and the loss in units of m, the substep's largest change (a fixed point, m = 0, has q = p = y)
+    float scale = b, loss_unit = b;
+    gell_status st = GELL_OK;
+    if (S->input_kind == 1) {
+        if ((st = delta_input(c, sub, S, &scale)) != GELL_OK) return st;
+        loss_unit = scale > 0.f ? scale : b;
+    }
+    st = lod_solver(c, sub, S->substeps);
     if (st != GELL_OK) return st;
     GELL_CUDA(c, cudaMemcpyAsync(T->tgt, Su.p, fb, cudaMemcpyDeviceToDevice, c->stream));
     GELL_CUDA(c, cudaMemcpyAsync(Su.p, S->backup, fb, cudaMemcpyDeviceToDevice, c->stream));
 
     // forward, every activation kept
     const int pb = blocks_for(c->nvox, 256);
-    GELL_KERNEL(c, "k_pack_input", (k_pack_input<<<pb < 148 * 16 ? pb : 148 * 16, 256, 0, c->stream>>>(
-                                        Su.p, Su.rate, c->g, 1.f / b, S->rate_scale, S->in)));
+    if (S->input_kind == 0)
+        GELL_KERNEL(c, "k_pack_input", (k_pack_input<<<pb < 148 * 16 ? pb : 148 * 16, 256, 0, c->stream>>>(
+                                            Su.p, Su.rate, c->g, 1.f / b, S->rate_scale, S->in)));
     st = launch_conv<2, 32, kRelu>(c, "k_conv3_in", S->map_in, S->w[0], S->bias[0], T->hb[0], nullptr, nullptr, nullptr,
                                    nullptr, 0.f, 0.f);
     for (int k = 0; k < 4 && st == GELL_OK; ++k) {
@@ -1174,13 +1236,13 @@ static gell_status train_pair(gell_ctx* c, int sub, SurrogateState* S, float lr,
     }
     if (st == GELL_OK)
         st = launch_conv<4, 16, kField>(c, "k_conv3_out", T->mh[4], S->w[9], S->bias[9], nullptr, nullptr, nullptr, S->ph,
-                                        Su.p, b, b);
+                                        Su.p, scale, b);
     if (st != GELL_OK) return st;
 
     // loss and its gradient
     const long long inner = (long long)(c->g.N - 4) * (c->g.N - 4) * (c->g.N - 4);
     const int lb = 148 * 8;
-    GELL_KERNEL(c, "k_loss_grad", (k_loss_grad<<<lb, 256, 0, c->stream>>>(S->ph, T->tgt, c->g, b, 1.f / (float)inner, T->gd,
+    GELL_KERNEL(c, "k_loss_grad", (k_loss_grad<<<lb, 256, 0, c->stream>>>(S->ph, T->tgt, c->g, loss_unit, 1.f / (float)inner, T->gd,
                                                                           T->scal + 2)));
     GELL_KERNEL(c, "k_sum_partials", (k_sum_partials<<<1, 32, 0, c->stream>>>(T->scal + 2, lb, 1, 1, T->scal + 1)));
 
@@ -1248,6 +1310,7 @@ gell_status gell_surrogate_load(gell_ctx* c, int sub, const float* weights, long
     S->substeps = substeps;
     S->rate_scale = rate_scale;
     S->threshold = threshold;
+    S->input_kind = c->sur_input;
     const float* W = weights;
     for (int l = 0; l < kLayers; ++l) {
         const LayerShape& s = kShape[l];
@@ -1277,7 +1340,9 @@ gell_status gell_surrogate_load(gell_ctx* c, int sub, const float* weights, long
             cudaMallocHost(&S->hmax, 4) != cudaSuccess)
             return fail(c, GELL_ERR_ALLOC, "surrogate activations (10 planes of 16 bytes per voxel)");
         GELL_CUDA(c, cudaMemsetAsync(S->in, 0, 2 * plane, c->stream));
-        gell_status st = plane_map(c, &S->map_in, S->in, 2);
+        gell_status st = GELL_OK;
+        if (cudaMalloc(&S->p0, field) != cudaSuccess) return fail(c, GELL_ERR_ALLOC, "surrogate field copy");
+        st = plane_map(c, &S->map_in, S->in, 2);
         if (st == GELL_OK) st = plane_map(c, &S->map_h, S->h, 4);
         if (st == GELL_OK) st = plane_map(c, &S->map_t, S->t, 4);
         if (st != GELL_OK) return st;

@@ -13,8 +13,10 @@ boundary value by a few hundred plain substeps, and each pair is one block of th
 a few mechanics steps (FM_update) move the cells, PreLOD rebuilds the uptake map, and the field
 before and after `substeps` plain substeps form the pair.
 
-Weight file: 8-byte magic b"GSUR0001", int32 substeps, float32 rate_scale, float32 threshold,
-int64 count, then `count` float32 weights in gell_surrogate_load's order (little-endian).
+Weight file: 8-byte magic b"GSUR0002", int32 substeps, float32 rate_scale, float32 threshold,
+int32 input_kind (GELL_OPT_SURROGATE_INPUT: 0 the field, 1 the change of one plain substep),
+int64 count, then `count` float32 weights in gell_surrogate_load's order (little-endian).  Files
+with the magic b"GSUR0001" have no input_kind (the field form).
 """
 from __future__ import annotations
 
@@ -23,7 +25,8 @@ from dataclasses import dataclass
 
 import numpy as np
 
-MAGIC = b"GSUR0001"
+MAGIC = b"GSUR0002"
+MAGIC_V1 = b"GSUR0001"
 # weights fitted for oxygen (the large workload's parameters) on 256^3 grids of 10 um
 DEFAULT_WEIGHTS = __import__("os").path.join(__import__("os").path.dirname(__file__), "data", "o2_surrogate_256.gsur")
 SHAPES = [(3, 32)] + [(32, 32)] * 8 + [(32, 1)]  # (cin, cout) of the ten convolutions
@@ -35,25 +38,31 @@ class SurrogateWeights:
     substeps: int = 50
     rate_scale: float = 0.1
     threshold: float = 1e-3
+    input_kind: int = 0
 
 
 def save_weights(path: str, sw: SurrogateWeights) -> None:
     w = np.ascontiguousarray(sw.weights, np.float32).reshape(-1)
     with open(path, "wb") as f:
         f.write(MAGIC)
-        f.write(struct.pack("<iffq", sw.substeps, sw.rate_scale, sw.threshold, w.size))
+        f.write(struct.pack("<iffiq", sw.substeps, sw.rate_scale, sw.threshold, sw.input_kind, w.size))
         f.write(w.astype("<f4").tobytes())
 
 
 def load_weights(path: str) -> SurrogateWeights:
     with open(path, "rb") as f:
-        if f.read(8) != MAGIC:
+        magic = f.read(8)
+        if magic == MAGIC:
+            substeps, rate_scale, threshold, input_kind, n = struct.unpack("<iffiq", f.read(24))
+        elif magic == MAGIC_V1:
+            substeps, rate_scale, threshold, n = struct.unpack("<iffq", f.read(20))
+            input_kind = 0
+        else:
             raise ValueError(f"{path}: not a surrogate weight file")
-        substeps, rate_scale, threshold, n = struct.unpack("<iffq", f.read(20))
         w = np.frombuffer(f.read(4 * n), "<f4").astype(np.float32)
     if w.size != n:
         raise ValueError(f"{path}: truncated")
-    return SurrogateWeights(w, substeps, rate_scale, threshold)
+    return SurrogateWeights(w, substeps, rate_scale, threshold, input_kind)
 
 
 def weight_count() -> int:
@@ -154,12 +163,13 @@ def sim_boundary(gb) -> float:
 def train(N: int = 256, pairs: int = 2000, substeps: int = 50, rate_scale: float = 0.1, seed: int = 11,
           cells: tuple[int, int] = (150_000, 450_000), lr: float = 3e-4, max_seconds: float = float("inf"),
           blocks: int = 4, warm: tuple[int, int] = (300, 1000), moves: tuple[int, int] = (1, 5),
-          log=print) -> SurrogateWeights:
+          input_kind: int = 0, log=print) -> SurrogateWeights:
     """Fit the operator with the library's training kernels (gell_surrogate_train_pair): one pair per
     step, never reused, from one context that follows a seeded spheroid for `blocks` blocks (each
     block: 1-5 mechanics steps, PreLOD, the pair) before the next spheroid replaces it.  Adam with
     the gradient clipped to norm 1 and the rate on a cosine from `lr` to 0; the loss is the mean
-    squared error inside the shell in units of the boundary value.  Stops after `max_seconds`."""
+    squared error inside the shell in units of the boundary value (input_kind 0) or of the largest
+    one-substep change (input_kind 1, GELL_OPT_SURROGATE_INPUT).  Stops after `max_seconds`."""
     import math
     import time
 
@@ -170,7 +180,7 @@ def train(N: int = 256, pairs: int = 2000, substeps: int = 50, rate_scale: float
     done = 0
     with gb.Simulation(voxel_num=N, voxel_length=10.0, max_cell_num=cells[1]) as sim:
         sim.add_substrate(gb.oxygen())
-        sim.surrogate_train_init(0, init_weights(seed), substeps, rate_scale)
+        sim.surrogate_train_init(0, init_weights(seed), substeps, rate_scale, input_kind)
         left = 0
         for it in range(pairs):
             if left == 0:
@@ -191,7 +201,7 @@ def train(N: int = 256, pairs: int = 2000, substeps: int = 50, rate_scale: float
                 break
         w = sim.surrogate_train_read(0, 0)
     log(f"fit: {done} pairs in {time.time() - t0:.1f} s")
-    return SurrogateWeights(w, substeps, rate_scale, 0.0)
+    return SurrogateWeights(w, substeps, rate_scale, 0.0, input_kind)
 
 
 def calibrate(sw: SurrogateWeights, N: int = 256, pairs: int = 64, seed: int = 1234,
@@ -212,7 +222,7 @@ def calibrate(sw: SurrogateWeights, N: int = 256, pairs: int = 64, seed: int = 1
     try:
         with gb.Simulation(voxel_num=N, voxel_length=10.0, max_cell_num=cells[1]) as sim:
             sim.add_substrate(gb.oxygen())
-            sim.surrogate_load(0, sw.weights, sw.substeps, sw.rate_scale, 1e30)
+            sim.surrogate_load(0, sw.weights, sw.substeps, sw.rate_scale, 1e30, sw.input_kind)
             for _ in range(pairs):
                 i = src.k % len(src.sims)
                 p, rate, tgt = src.next()
@@ -247,7 +257,7 @@ def time_inference(N: int = 128, reps: int = 3, ring: bool = True, path: str | N
         sim.PreLOD()
         sim.LODsolver(100, 0)
         sim.set_conv_ring(ring)
-        sim.surrogate_load(0, sw.weights, sw.substeps, sw.rate_scale, sw.threshold)
+        sim.surrogate_load(0, sw.weights, sw.substeps, sw.rate_scale, sw.threshold, sw.input_kind)
         sim.surrogate_infer(0)  # first launches (module loading) outside the timing
         sim.profile(True)
         sim.profile_read(reset=True)
@@ -272,7 +282,7 @@ def time_training(N: int = 128, reps: int = 2, cells: int = 40_000, log=print) -
         sim.import_cells(c)
         sim.PreLOD()
         sim.LODsolver(100, 0)
-        sim.surrogate_train_init(0, sw.weights, sw.substeps, sw.rate_scale)
+        sim.surrogate_train_init(0, sw.weights, sw.substeps, sw.rate_scale, sw.input_kind)
         sim.surrogate_train_pair(0, 1e-5)  # first launches (module loading) outside the timing
         sim.profile(True)
         sim.profile_read(reset=True)
@@ -342,11 +352,16 @@ def main(argv=None) -> int:
     ap.add_argument("--lr", type=float, default=3e-4)
     ap.add_argument("--tol", type=float, default=0.01)
     ap.add_argument("--max-seconds", type=float, default=float("inf"))
+    ap.add_argument("--input", choices=("field", "delta"), default="field",
+                    help="the operator's input: the field p / b, or the change of one plain substep")
+    ap.add_argument("--margin", type=float, default=1.1, help="calibration safety margin")
     a = ap.parse_args(argv)
-    sw = train(a.N, a.pairs, a.substeps, lr=a.lr, max_seconds=a.max_seconds,
+    sw = train(a.N, a.pairs, a.substeps, lr=a.lr, max_seconds=a.max_seconds, input_kind=int(a.input == "delta"),
                log=lambda m: print(m, flush=True))
     t1 = time.time()
-    sw.threshold, pts = calibrate(sw, a.N, a.val_pairs, tol=a.tol, log=lambda m: print(m, flush=True))
+    # the judge is calibrated on the regime the surrogate stands in for: quasi-steady fields
+    sw.threshold, pts = calibrate(sw, a.N, a.val_pairs, tol=a.tol, log=lambda m: print(m, flush=True),
+                                  warm=(800, 1500), moves=(1, 1), margin=a.margin)
     print(f"calibration: {a.val_pairs} pairs in {time.time() - t1:.1f} s", flush=True)
     save_weights(a.out, sw)
     return 0

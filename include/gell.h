@@ -284,7 +284,8 @@ enum {
     GELL_OPT_CONV_RING = 4,
     GELL_OPT_SWEEP_RING = 5,
     GELL_OPT_SWEEP_L2HINT = 6,
-    GELL_OPT_SWEEP_RING_LAG = 7
+    GELL_OPT_SWEEP_RING_LAG = 7,
+    GELL_OPT_SURROGATE_INPUT = 9
 };
 /* GELL_OPT_SWEEP_RING (-1..8, default -1): 1 runs the LOD sweeps as ring kernels (a few group
  * slots of shared memory per warp; back substitution re-reads each group from L2 and recomputes its
@@ -294,7 +295,13 @@ enum {
  * GELL_OPT_SWEEP_L2HINT (0 or 1, default 0): the ring sweeps load groups they will read again with
  * priority to stay in L2.  GELL_OPT_SWEEP_RING_LAG (0..7, default 0 = 1): how many of its own
  * result stores a ring warp lets run before it refills a stored slot (capped at the slots less
- * one).  Results are identical for every value of these options. */
+ * one).  Results are identical for every value of these options.
+ * GELL_OPT_SURROGATE_INPUT (0 or 1, default 0), for surrogates loaded (or trained) after it is set:
+ * 0 gives the operator the field p / b and scales its output d by b (q = p + b d); 1 gives it the
+ * change of one plain substep, (L(p) - p) / m with m its largest magnitude inside the shell, and
+ * scales the output by m (q = p + m d).  A LOD substep is affine in the field, so the change over
+ * the surrogate's substeps is a linear function of that one-substep change; in this form bf16
+ * inputs quantise the change rather than the field.  Weights are trained for one form. */
 /* GELL_OPT_CONV_RING (0 or 1, default 1): the surrogate's convolutions keep the input rows of
  * consecutive lines in a ring of shared-memory slots (each row read from L2 once per unit of 32
  * lines) instead of loading all nine rows per tile; the results are the same. */

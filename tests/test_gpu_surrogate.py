@@ -114,6 +114,42 @@ def test_surrogate_layers_match_torch(N, ring):
         sim.sync()
 
 
+def test_delta_input_planes_and_output():
+    """The delta form (GELL_OPT_SURROGATE_INPUT = 1): channel 0 of the input is the change of one
+    plain substep over its largest magnitude m inside the shell (0 on the shell), the field is left
+    as it was, and the output is p + m d inside the shell, b on it."""
+    N = 40
+    w = random_weights(7)
+    Ws = layer_params(w)
+    with make_sim(N, 8) as sim:
+        b = 38.0
+        p = sim.field(0)
+        sim.LODsolver(1, 0)
+        p1 = sim.field(0)
+        sim.set_field(0, p)
+        g = np.arange(N)
+        sh = (g < 2) | (g > N - 3)
+        shell = (sh[:, None, None] | sh[None, :, None] | sh[None, None, :]).ravel()
+        m = np.float32(np.abs(p1 - p)[~shell].max())
+        sim.surrogate_load(0, w, 50, 0.1, 1.0, input_kind=1)
+        sim.surrogate_run_layers(0, 0)
+        x = sim.surrogate_read(0, 0)[:3]
+        bf = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(torch.bfloat16).float().numpy()
+        d1 = np.where(shell, np.float32(0), (p1 - p) * (np.float32(1) / m)).astype(np.float32)
+        assert np.array_equal(x[0], bf(d1))
+        assert np.array_equal(x[1], bf(sim.dump_rate(0) * np.float32(0.1)))
+        assert np.array_equal(x[2], shell.astype(np.float32))
+        assert np.array_equal(sim.field(0).view(np.uint32), p.view(np.uint32))
+        sim.surrogate_run_layers(0, 9)
+        h_in = sim.surrogate_read(0, 1)
+        sim.surrogate_run_layers(0, 10)
+        d = conv(h_in, Ws[9], N)[0]
+        ref = np.where(shell, np.float32(b), p + m * d)
+        got = sim.surrogate_read(0, 3)
+        assert np.abs(got - ref).max() <= 1e-5 * b, np.abs(got - ref).max()
+        sim.sync()
+
+
 def test_judge_accepts_and_falls_back():
     N, K = 48, 50
     w = random_weights(4)

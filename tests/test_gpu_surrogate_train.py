@@ -39,8 +39,10 @@ def make_sim(N, seed, cells=2000):
     return sim
 
 
-def torch_grads(w, x, p, y, N, b=38.0):
-    """Loss and flat gradient of the operator in fp32, activations rounded to bf16 on the way."""
+def torch_grads(w, x, p, y, N, b=38.0, scale=None):
+    """Loss and flat gradient of the operator in fp32, activations rounded to bf16 on the way.  The
+    output is q = p + scale * d and the loss is in units of `scale` (default: b, the field form)."""
+    scale = b if scale is None else scale
     dev = torch.device("cuda")
 
     def rnd(t):  # stored as bf16, gradient passed straight through
@@ -68,8 +70,8 @@ def torch_grads(w, x, p, y, N, b=38.0):
     inner = torch.from_numpy(~(sh[:, None, None] | sh[None, :, None] | sh[None, None, :]).ravel()).to(dev)
     pt = torch.from_numpy(p).to(dev)
     yt = torch.from_numpy(y).to(dev)
-    q = pt + b * d
-    e = ((q - yt) / b)[inner]
+    q = pt + scale * d
+    e = ((q - yt) / scale)[inner]
     loss = (e * e).mean()
     loss.backward()
     flat = torch.cat([(prm.grad if prm.grad is not None else torch.zeros_like(prm)).reshape(-1) for prm in params])
@@ -123,3 +125,34 @@ def test_training_reduces_loss_on_a_pair():
         sim.sync()
     print("losses", losses[0], losses[-1])
     assert losses[-1] < 0.6 * losses[0]
+
+
+@pytest.mark.parametrize("N", [40, 37])
+def test_training_gradient_matches_autograd_delta_input(N):
+    """The delta form (GELL_OPT_SURROGATE_INPUT = 1): the input is the change of one plain substep
+    over its largest magnitude m, the output q = p + m d, the loss in units of m."""
+    w = random_weights(23)
+    with make_sim(N, 11) as sim:
+        p = sim.field(0)
+        sim.LODsolver(1, 0)
+        p1 = sim.field(0)
+        sim.set_field(0, p)
+        g = np.arange(N)
+        sh = (g < 2) | (g > N - 3)
+        inner = ~(sh[:, None, None] | sh[None, :, None] | sh[None, None, :]).ravel()
+        m = float(np.abs(p1 - p)[inner].max())
+        assert m > 0
+        sim.surrogate_train_init(0, w, 5, 0.1, input_kind=1)
+        loss = sim.surrogate_train_pair(0, 0.0)
+        grad = sim.surrogate_train_read(0, 1)
+        y = sim.surrogate_train_read(0, 2)
+        x = sim.surrogate_read(0, 0)[:3]
+        assert np.array_equal(sim.field(0).view(np.uint32), y.view(np.uint32))
+        sim.sync()
+    tloss, tgrad = torch_grads(w, x, p, y, N, scale=np.float32(m))
+    assert abs(loss - tloss) <= 1e-3 * tloss, (loss, tloss)
+    for name, sl in layer_slices():
+        a, r = grad[sl].astype(np.float64), tgrad[sl].astype(np.float64)
+        rel = np.linalg.norm(a - r) / max(np.linalg.norm(r), 1e-30)
+        cos = float(a @ r / max(np.linalg.norm(a) * np.linalg.norm(r), 1e-30))
+        assert rel < 2e-2 and cos > 0.9995, (name, rel, cos)

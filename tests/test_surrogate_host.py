@@ -8,14 +8,25 @@ from gell_b200 import surrogate as gs
 
 def test_weight_file_round_trip(tmp_path):
     rng = np.random.default_rng(0)
-    sw = gs.SurrogateWeights(rng.standard_normal(gs.weight_count()).astype(np.float32), 50, 0.1, 2.35e-3)
-    path = tmp_path / "w.gsur"
-    gs.save_weights(str(path), sw)
+    for kind in (0, 1):
+        sw = gs.SurrogateWeights(rng.standard_normal(gs.weight_count()).astype(np.float32), 50, 0.1, 2.35e-3, kind)
+        path = tmp_path / f"w{kind}.gsur"
+        gs.save_weights(str(path), sw)
+        back = gs.load_weights(str(path))
+        assert (back.substeps, back.rate_scale, back.threshold, back.input_kind) == (50, np.float32(0.1),
+                                                                                     np.float32(2.35e-3), kind)
+        assert np.array_equal(back.weights, sw.weights)
+        raw = path.read_bytes()
+        assert raw[:8] == b"GSUR0002" and len(raw) == 8 + 24 + 4 * gs.weight_count()
+
+
+def test_version_one_weight_files_load_as_the_field_form(tmp_path):
+    import struct
+    w = np.arange(gs.weight_count(), dtype=np.float32)
+    path = tmp_path / "v1.gsur"
+    path.write_bytes(b"GSUR0001" + struct.pack("<iffq", 50, 0.1, 5e-3, w.size) + w.astype("<f4").tobytes())
     back = gs.load_weights(str(path))
-    assert (back.substeps, back.rate_scale, back.threshold) == (50, np.float32(0.1), np.float32(2.35e-3))
-    assert np.array_equal(back.weights, sw.weights)
-    raw = path.read_bytes()
-    assert raw[:8] == b"GSUR0001" and len(raw) == 8 + 20 + 4 * gs.weight_count()
+    assert back.input_kind == 0 and back.substeps == 50 and np.array_equal(back.weights, w)
 
 
 def test_weight_file_rejects_bad_input(tmp_path):
