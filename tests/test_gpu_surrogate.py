@@ -202,7 +202,7 @@ def test_packaged_surrogate_vs_fp64_oracle():
         sim.import_cells(cells)
         sim.PreLOD()
         sim.LODsolver(1000, 0)
-        sim.surrogate_load(0, sw.weights, sw.substeps, sw.rate_scale, sw.threshold)
+        sim.surrogate_load(0, sw.weights, sw.substeps, sw.rate_scale, sw.threshold, sw.input_kind)
         p = sim.field(0)
         rate = sim.dump_rate(0)
         ok, r = sim.lod_surrogate(0)
