@@ -543,11 +543,17 @@ __global__ void __launch_bounds__(64 * kMaxComputeWarps, 1) k_sweep(const __grid
     uint64_t* fb = full + warp * 32;
     uint64_t* eb = empty + warp * 32;
     int k = 0;
-    for (long long t = (long long)blockIdx.x * W + warp; t < total; t += step, ++k) {
-        const TileDesc d = tile_desc<AXIS>(a, t, per_sub);
+    long long t = (long long)blockIdx.x * W + warp;
+    if (t >= total) return;
+    // the next tile's description (for x: each lane's uptake flag, a global load) is requested one
+    // tile ahead, so its latency is not paid in front of the forward elimination
+    TileDesc d = tile_desc<AXIS>(a, t, per_sub);
+    for (; t < total; t += step, ++k) {
+        const TileDesc dn = t + step < total ? tile_desc<AXIS>(a, t + step, per_sub) : d;
         const bool ok = (k & 1) ? run_tile<AXIS, 1>(a, d, buf, fb, eb, sEFR, Na)
                                 : run_tile<AXIS, 0>(a, d, buf, fb, eb, sEFR, Na);
         if (!ok) break;
+        d = dn;
     }
 }
 
@@ -1017,8 +1023,11 @@ __global__ void __launch_bounds__(64 * kBatchWarps, 1) k_sweep_batch(const __gri
     uint64_t* eb = empty + warp * kBatchMaxGroups;
     uint32_t perm = perm_identity(), fph = 0;
     int item = 0, staged = -1;
+    BTile dnext = t_begin < t_end ? btile<AXIS>(a, t_begin, item) : BTile{};
     for (long long t = t_begin; t < t_end; ++t) {
-        const BTile d = btile<AXIS>(a, t, item);
+        // the next tile's description is requested one tile ahead (see k_sweep)
+        const BTile d = dnext;
+        if (t + 1 < t_end) dnext = btile<AXIS>(a, t + 1, item);
         const BatchItem& it = a.items[d.item];
         if (d.item != staged) {
             // E of the elements the reference's recurrences update; 0 elsewhere (identity)
