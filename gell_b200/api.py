@@ -400,6 +400,10 @@ class Simulation:
         """Result stores a ring-sweep warp lets run before refilling a stored slot (0 = default)."""
         self._check(self.lib.gell_set_option(self.h, 7, int(lag)), "gell_set_option")
 
+    def set_lod_streams(self, on: bool = True) -> None:
+        """Each substrate's LOD substeps on a stream of its own (same results)."""
+        self._check(self.lib.gell_set_option(self.h, 10, int(bool(on))), "gell_set_option")
+
     def set_sweep_l2hint(self, on: bool = True) -> None:
         """The ring sweeps' L2 eviction priorities (same results)."""
         self._check(self.lib.gell_set_option(self.h, 6, int(bool(on))), "gell_set_option")

@@ -197,6 +197,11 @@ static void free_all(gell_ctx* c) {
     for (auto e : c->ev_pool) cudaEventDestroy(e);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     if (c->xfer) cudaStreamDestroy(c->xfer);
+    for (int s = 0; s < 8; ++s) {
+        if (c->sub_stream[s]) cudaStreamDestroy(c->sub_stream[s]);
+        if (c->sub_join[s]) cudaEventDestroy(c->sub_join[s]);
+    }
+    if (c->sub_fork) cudaEventDestroy(c->sub_fork);
     if (c->cells_ev) cudaEventDestroy(c->cells_ev);
     if (c->xfer_ev) cudaEventDestroy(c->xfer_ev);
 }
@@ -683,6 +688,21 @@ gell_status gell_set_option(gell_ctx* c, int option, int64_t value) {
             c->sweep_ring = (int)value;
             return GELL_OK;
         case GELL_OPT_SWEEP_L2HINT: c->sweep_l2hint = value != 0; return GELL_OK;
+        case GELL_OPT_LOD_STREAMS:
+            c->lod_streams = value != 0;
+            // the streams exist before any capture that uses them
+            if (c->lod_streams && !c->sub_fork) {
+                bool ok = cudaEventCreateWithFlags(&c->sub_fork, cudaEventDisableTiming) == cudaSuccess;
+                for (int s = 1; ok && s < 8; ++s)
+                    ok = cudaStreamCreateWithFlags(&c->sub_stream[s], cudaStreamNonBlocking) == cudaSuccess &&
+                         cudaEventCreateWithFlags(&c->sub_join[s], cudaEventDisableTiming) == cudaSuccess;
+                if (!ok) {
+                    cudaGetLastError();
+                    c->lod_streams = false;
+                    return fail(c, GELL_ERR_CUDA, "substrate streams");
+                }
+            }
+            return GELL_OK;
         case GELL_OPT_SURROGATE_INPUT:
             if (value < 0 || value > 1) return fail(c, GELL_ERR_INVALID_ARG, "surrogate input outside 0..1");
             c->sur_input = (int)value;

@@ -1233,7 +1233,7 @@ gell_status prelod(gell_ctx* c, int sub) {
 // The ring sweeps (k_sweep_ring): W warps per CTA, each with R group slots, R as large as shared
 // memory allows (at most kRingMaxSlots, at least 2 unless a line is one group).
 static gell_status lod_solver_ring(gell_ctx* c, const LodArgs& ax, const LodArgs& ay, const LodArgs& az, int s0,
-                                   int s1, int substeps) {
+                                   int s1, int substeps, cudaStream_t strm) {
     const int ns = ax.nsub;
     const int N = c->g.N;
     const int B = (N + 31) / 32;
@@ -1293,15 +1293,15 @@ static gell_status lod_solver_ring(gell_ctx* c, const LodArgs& ax, const LodArgs
     sa.g = c->g;
     sa.dt = c->P.diffusion_dt;
     for (int k = 0; k < substeps; ++k) {
-        GELL_KERNEL(c, "k_source_lines", k_source_lines<<<num_sms() * 8, 256, 0, c->stream>>>(sa));
+        GELL_KERNEL(c, "k_source_lines", k_source_lines<<<num_sms() * 8, 256, 0, strm>>>(sa));
         if (hint) {
-            GELL_KERNEL(c, "k_sweep_x", k_sweep_ring<0, true><<<gx, W * 32, smem, c->stream>>>(ax, R, L));
-            GELL_KERNEL(c, "k_sweep_y", k_sweep_ring<1, true><<<gy, W * 32, smem, c->stream>>>(ay, R, L));
-            GELL_KERNEL(c, "k_sweep_z", k_sweep_ring<2, true><<<gz, W * 32, smem, c->stream>>>(az, R, L));
+            GELL_KERNEL(c, "k_sweep_x", k_sweep_ring<0, true><<<gx, W * 32, smem, strm>>>(ax, R, L));
+            GELL_KERNEL(c, "k_sweep_y", k_sweep_ring<1, true><<<gy, W * 32, smem, strm>>>(ay, R, L));
+            GELL_KERNEL(c, "k_sweep_z", k_sweep_ring<2, true><<<gz, W * 32, smem, strm>>>(az, R, L));
         } else {
-            GELL_KERNEL(c, "k_sweep_x", k_sweep_ring<0, false><<<gx, W * 32, smem, c->stream>>>(ax, R, L));
-            GELL_KERNEL(c, "k_sweep_y", k_sweep_ring<1, false><<<gy, W * 32, smem, c->stream>>>(ay, R, L));
-            GELL_KERNEL(c, "k_sweep_z", k_sweep_ring<2, false><<<gz, W * 32, smem, c->stream>>>(az, R, L));
+            GELL_KERNEL(c, "k_sweep_x", k_sweep_ring<0, false><<<gx, W * 32, smem, strm>>>(ax, R, L));
+            GELL_KERNEL(c, "k_sweep_y", k_sweep_ring<1, false><<<gy, W * 32, smem, strm>>>(ay, R, L));
+            GELL_KERNEL(c, "k_sweep_z", k_sweep_ring<2, false><<<gz, W * 32, smem, strm>>>(az, R, L));
         }
     }
     return GELL_OK;
@@ -1317,10 +1317,9 @@ static bool ring_by_default(const gell_ctx* c, int ns) {
     return (227 * 1024 - fixed) / (B * kSlotFloats * 4) < 4;
 }
 
-gell_status lod_solver(gell_ctx* c, int sub, int substeps) {
-    if (c->subs.empty() || substeps == 0) return GELL_OK;
+// LOD substeps of substrates [s0, s1) on stream `strm`.
+static gell_status lod_solver_range(gell_ctx* c, int s0, int s1, int substeps, cudaStream_t strm) {
     LodArgs ax{}, ay{}, az{};
-    int s0 = sub < 0 ? 0 : sub, s1 = sub < 0 ? (int)c->subs.size() : sub + 1;
     int ns = 0;
     for (int s = s0; s < s1; ++s, ++ns) {
         const Substrate& S = c->subs[s];
@@ -1346,7 +1345,7 @@ gell_status lod_solver(gell_ctx* c, int sub, int substeps) {
     const int Na = (N + 31) & ~31;
     const int smem_cap = 227 * 1024;
     if (c->sweep_ring > 0 || (c->sweep_ring < 0 && ring_by_default(c, ns)))
-        return lod_solver_ring(c, ax, ay, az, s0, s1, substeps);
+        return lod_solver_ring(c, ax, ay, az, s0, s1, substeps, strm);
     const int fixed = 1024 + align128(ns * Na * 4) + 2 * 8 * 32 * 8;
     int w = (smem_cap - fixed) / (B * kSlotFloats * 4);
     w = w > kMaxComputeWarps ? kMaxComputeWarps : w;
@@ -1391,10 +1390,10 @@ gell_status lod_solver(gell_ctx* c, int sub, int substeps) {
     sa.g = c->g;
     sa.dt = c->P.diffusion_dt;
     for (int k = 0; k < substeps; ++k) {
-        GELL_KERNEL(c, "k_source_lines", k_source_lines<<<num_sms() * 8, 256, 0, c->stream>>>(sa));
-        GELL_KERNEL(c, "k_sweep_x", k_sweep<0><<<gx, w * 64, smem, c->stream>>>(ax));
-        GELL_KERNEL(c, "k_sweep_y", k_sweep<1><<<gy, w * 64, smem, c->stream>>>(ay));
-        GELL_KERNEL(c, "k_sweep_z", k_sweep<2><<<gz, w * 64, smem, c->stream>>>(az));
+        GELL_KERNEL(c, "k_source_lines", k_source_lines<<<num_sms() * 8, 256, 0, strm>>>(sa));
+        GELL_KERNEL(c, "k_sweep_x", k_sweep<0><<<gx, w * 64, smem, strm>>>(ax));
+        GELL_KERNEL(c, "k_sweep_y", k_sweep<1><<<gy, w * 64, smem, strm>>>(ay));
+        GELL_KERNEL(c, "k_sweep_z", k_sweep<2><<<gz, w * 64, smem, strm>>>(az));
     }
     return GELL_OK;
 }
@@ -1502,6 +1501,45 @@ gell_status lod_batch_run(LodBatch* b, cudaStream_t st, int substeps) {
         GELL_KERNEL(c, "k_sweep_x", k_sweep_batch<0><<<grid(a.total[0]), W * 64, smem, st>>>(a, b->Bmax));
         GELL_KERNEL(c, "k_sweep_y", k_sweep_batch<1><<<grid(a.total[1]), W * 64, smem, st>>>(a, b->Bmax));
         GELL_KERNEL(c, "k_sweep_z", k_sweep_batch<2><<<grid(a.total[2]), W * 64, smem, st>>>(a, b->Bmax));
+    }
+    return GELL_OK;
+}
+
+// A stream per substrate (GELL_OPT_LOD_STREAMS): the substrates' substeps are independent chains,
+// so on separate streams one sweep's ramp-up and drain (an SM whose last tile is done while others
+// still work) overlap another substrate's sweep instead of idling the GPU between launches.
+static bool substrate_streams(gell_ctx* c, int s0, int s1) {
+    if (!c->lod_streams || s1 - s0 < 2 || c->prof_on) return false;
+    for (int s = s0 + 1; s < s1; ++s) {
+        if (c->sub_stream[s]) continue;
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(c->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return false;
+        if (cudaStreamCreateWithFlags(&c->sub_stream[s], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&c->sub_join[s], cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+    }
+    if (!c->sub_fork && cudaEventCreateWithFlags(&c->sub_fork, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return true;
+}
+
+gell_status lod_solver(gell_ctx* c, int sub, int substeps) {
+    if (c->subs.empty() || substeps == 0) return GELL_OK;
+    const int s0 = sub < 0 ? 0 : sub, s1 = sub < 0 ? (int)c->subs.size() : sub + 1;
+    if (!substrate_streams(c, s0, s1)) return lod_solver_range(c, s0, s1, substeps, c->stream);
+    GELL_CUDA(c, cudaEventRecord(c->sub_fork, c->stream));
+    for (int s = s0 + 1; s < s1; ++s) GELL_CUDA(c, cudaStreamWaitEvent(c->sub_stream[s], c->sub_fork, 0));
+    for (int s = s0; s < s1; ++s) {
+        gell_status st = lod_solver_range(c, s, s + 1, substeps, s == s0 ? c->stream : c->sub_stream[s]);
+        if (st != GELL_OK) return st;
+    }
+    for (int s = s0 + 1; s < s1; ++s) {
+        GELL_CUDA(c, cudaEventRecord(c->sub_join[s], c->sub_stream[s]));
+        GELL_CUDA(c, cudaStreamWaitEvent(c->stream, c->sub_join[s], 0));
     }
     return GELL_OK;
 }

@@ -97,3 +97,34 @@ def test_ring_slot_counts_and_l2_hints_give_the_same_fields(N):
         got = run(N, cells, field, 2, ring=ring, hint=hint, lag=lag)
         for sub in range(2):
             assert bits_equal(got[sub], exp[sub]), (N, ring, hint, lag, sub)
+
+
+@pytest.mark.parametrize("N,ring", [(131, 0), (400, 0), (600, 1)])
+def test_a_stream_per_substrate_gives_the_same_fields(N, ring):
+    """GELL_OPT_LOD_STREAMS: each substrate's substeps on a stream of its own, eagerly and replayed
+    from the step graph (gell_run_mechanics), bit for bit the single-stream fields."""
+    lo, hi = N // 3, N // 3 + N // 6
+    cells = one_per_voxel(N, 10.0, seed=N + 31, lo=lo, hi=hi)
+    rng = np.random.Generator(np.random.Philox(N + 32))
+    field = rng.uniform(10.0, 38.0, N ** 3).astype(np.float32)
+    out = []
+    for streams in (False, True):
+        with gb.Simulation(voxel_num=N, voxel_length=10.0, max_cell_num=len(cells) + 1024) as sim:
+            sim.add_substrate(gb.oxygen())
+            sim.add_substrate(gb.drug())
+            sim.set_sweep_ring(ring if ring else -1)
+            sim.set_lod_streams(streams)
+            sim.set_field(0, field)
+            sim.set_field(1, field * np.float32(0.03))
+            sim.import_cells(cells)
+            sim.PreLOD()
+            sim.LODsolver(2)
+            first = (sim.field(0), sim.field(1))
+            sim.run_mechanics(4, 3)
+            sim.sync()
+            out.append((first, (sim.field(0), sim.field(1)), sim.export_cells()))
+    for sub in range(2):
+        assert bits_equal(out[0][0][sub], out[1][0][sub]), (N, sub)
+        # after the cells move, several can share a voxel: float-atomic uptake sums (1e-5)
+        np.testing.assert_allclose(out[0][1][sub], out[1][1][sub], rtol=1e-5, atol=0)
+    assert np.array_equal(out[0][2].view(np.uint8), out[1][2].view(np.uint8))
