@@ -475,6 +475,19 @@ gell_status gell_substrate_add(gell_ctx* c, const gell_substrate* s, int* index_
     if (index_out) *index_out = (int)c->subs.size() - 1;
     // rate maps of the existing substrates stay; rebuild all on the next prelod
     GELL_CUDA(c, cudaStreamSynchronize(c->stream));
+    // a second substrate: create the substrate streams now, before any graph capture uses them
+    if (c->lod_streams && c->subs.size() >= 2) {
+        const int s = (int)c->subs.size() - 1;
+        if (s < 8 && !c->sub_stream[s]) {
+            bool ok = (c->sub_fork || cudaEventCreateWithFlags(&c->sub_fork, cudaEventDisableTiming) == cudaSuccess) &&
+                      cudaStreamCreateWithFlags(&c->sub_stream[s], cudaStreamNonBlocking) == cudaSuccess &&
+                      cudaEventCreateWithFlags(&c->sub_join[s], cudaEventDisableTiming) == cudaSuccess;
+            if (!ok) {
+                cudaGetLastError();
+                c->lod_streams = 0;  // fall back to one stream
+            }
+        }
+    }
     return GELL_OK;
 }
 
@@ -691,11 +704,12 @@ gell_status gell_set_option(gell_ctx* c, int option, int64_t value) {
         case GELL_OPT_LOD_STREAMS:
             c->lod_streams = value != 0;
             // the streams exist before any capture that uses them
-            if (c->lod_streams && !c->sub_fork) {
-                bool ok = cudaEventCreateWithFlags(&c->sub_fork, cudaEventDisableTiming) == cudaSuccess;
-                for (int s = 1; ok && s < 8; ++s)
-                    ok = cudaStreamCreateWithFlags(&c->sub_stream[s], cudaStreamNonBlocking) == cudaSuccess &&
-                         cudaEventCreateWithFlags(&c->sub_join[s], cudaEventDisableTiming) == cudaSuccess;
+            if (c->lod_streams) {
+                bool ok = c->sub_fork || cudaEventCreateWithFlags(&c->sub_fork, cudaEventDisableTiming) == cudaSuccess;
+                for (int s = 1; ok && s < (int)c->subs.size() && s < 8; ++s)
+                    if (!c->sub_stream[s])
+                        ok = cudaStreamCreateWithFlags(&c->sub_stream[s], cudaStreamNonBlocking) == cudaSuccess &&
+                             cudaEventCreateWithFlags(&c->sub_join[s], cudaEventDisableTiming) == cudaSuccess;
                 if (!ok) {
                     cudaGetLastError();
                     c->lod_streams = false;

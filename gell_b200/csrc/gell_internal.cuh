@@ -122,7 +122,7 @@ struct gell_ctx {
     int sweep_ring = -1;       // GELL_OPT_SWEEP_RING: -1 auto, 0 line tiles, 1 ring, >= 2 ring of at most that many slots
     bool sweep_l2hint = false;  // GELL_OPT_SWEEP_L2HINT: the ring sweeps' L2 eviction priorities
     int sweep_ring_lag = 0;     // GELL_OPT_SWEEP_RING_LAG: stores in flight per ring warp (0: default)
-    int lod_streams = 0;        // GELL_OPT_LOD_STREAMS: a stream per substrate for the LOD substeps
+    int lod_streams = 1;        // GELL_OPT_LOD_STREAMS: a stream per substrate for the LOD substeps
     cudaStream_t sub_stream[8] = {};
     cudaEvent_t sub_join[8] = {};
     cudaEvent_t sub_fork = nullptr;

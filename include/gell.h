@@ -303,9 +303,9 @@ enum {
  * scales the output by m (q = p + m d).  A LOD substep is affine in the field, so the change over
  * the surrogate's substeps is a linear function of that one-substep change; in this form bf16
  * inputs quantise the change rather than the field.  Weights are trained for one form.
- * GELL_OPT_LOD_STREAMS (0 or 1, default 0): the LOD substeps of each substrate run on a stream of
- * their own (forked from and joined back to the context's stream), so that the sweeps of different
- * substrates overlap.  Results are identical. */
+ * GELL_OPT_LOD_STREAMS (0 or 1, default 1): the LOD substeps of each substrate run on a stream of
+ * their own (forked from and joined back to the context's stream), so that one substrate's sweep
+ * fills the SMs another's leaves idle at its start and end.  Results are identical. */
 /* GELL_OPT_CONV_RING (0 or 1, default 1): the surrogate's convolutions keep the input rows of
  * consecutive lines in a ring of shared-memory slots (each row read from L2 once per unit of 32
  * lines) instead of loading all nine rows per tile; the results are the same. */
