@@ -823,13 +823,18 @@ __device__ __forceinline__ long long tile_at_cost(const BatchArgs& a, long long 
 }
 
 __device__ __forceinline__ uint32_t perm_get(uint32_t perm, int g) { return (perm >> (4 * g)) & 15u; }
-// next tile's permutation: the first B entries reversed, the rest kept
-__device__ __forceinline__ uint32_t perm_next(uint32_t perm, int B) {
-    uint32_t out = perm;
-    for (int j = 0; j < B; ++j) {
-        out &= ~(15u << (4 * j));
-        out |= perm_get(perm, B - 1 - j) << (4 * j);
-    }
+// Slots of the next tile (Bn groups) after a tile of B groups: first the slots this tile leaves
+// unused (ascending; the producer fills them as soon as the tile starts, so a short tile's successor
+// is loaded a whole tile ahead), then the slots this tile frees, in the order its back substitution
+// frees them (top group first).
+__device__ __forceinline__ uint32_t batch_perm_next(uint32_t perm, int B, int Bn, int Bmax) {
+    uint32_t used = 0;
+    for (int g = 0; g < B; ++g) used |= 1u << perm_get(perm, g);
+    uint32_t out = 0;
+    int j = 0;
+    for (int sl = 0; sl < Bmax && j < Bn; ++sl)
+        if (!((used >> sl) & 1u)) out |= (uint32_t)sl << (4 * j++);
+    for (int g = B - 1; g >= 0 && j < Bn; --g) out |= perm_get(perm, g) << (4 * j++);
     return out;
 }
 __device__ __forceinline__ uint32_t perm_identity() {
@@ -934,9 +939,7 @@ __device__ __forceinline__ bool batch_tile(const BatchArgs& a, const BatchItem& 
 
 template <int AXIS>
 __device__ void batch_producer(const BatchArgs& a, float* buf, uint64_t* full, uint64_t* empty, long long t,
-                               long long t_end) {
-    const long long step = 1;
-    const long long total = t_end;
+                               long long t_end, int Bmax) {
     int item = 0;
     BTile d = btile<AXIS>(a, t, item);
     uint32_t perm = perm_identity(), eph = 0;
@@ -947,12 +950,23 @@ __device__ void batch_producer(const BatchArgs& a, float* buf, uint64_t* full, u
     for (;;) {
         const BatchItem& it = a.items[d.item];
         const int B = it.B;
-        const long long tn = t + step;
-        const bool has_next = tn < total;
+        const long long tn = t + 1;
+        const bool has_next = tn < t_end;
         int itemn = item;
         const BTile dn = has_next ? btile<AXIS>(a, tn, itemn) : d;
         const BatchItem& itn = a.items[dn.item];
         const int Bn = has_next ? itn.B : 0;
+        const uint32_t permn = has_next ? batch_perm_next(perm, B, Bn, Bmax) : 0u;
+        // the next tile's first groups into the slots this tile leaves unused (every store has read
+        // its slot: the previous tile ended with a full wait)
+        int nxt = 0;
+        uint32_t used = 0;
+        for (int g = 0; g < B; ++g) used |= 1u << perm_get(perm, g);
+        for (int sl = 0; sl < Bmax && nxt < Bn; ++sl)
+            if (!((used >> sl) & 1u)) {
+                bbox_load<AXIS>(itn, dn, nxt, buf + (size_t)sl * kSlotFloats, full + sl);
+                ++nxt;
+            }
         for (int g = B - 1; g >= 0; --g) {
             const int s = (int)perm_get(perm, g);
             if (!mbar_wait1(empty + s, (eph >> s) & 1u, a.err, 8 + AXIS)) {
@@ -962,24 +976,22 @@ __device__ void batch_producer(const BatchArgs& a, float* buf, uint64_t* full, u
             eph ^= 1u << s;
             bbox_store<AXIS>(it, d, g, buf + (size_t)s * kSlotFloats);
             bulk_commit();
-            if (has_next && g + 1 <= B - 1 && B - 2 - g < Bn) {
-                // the store of group g+1 has read its slot: it takes the next tile's group B-2-g
+            if (g + 1 <= B - 1 && nxt < Bn) {
+                // the store of group g+1 has read its slot: it takes the next tile's next group
                 bulk_wait_read<1>();
                 const int s1 = (int)perm_get(perm, g + 1);
-                bbox_load<AXIS>(itn, dn, B - 2 - g, buf + (size_t)s1 * kSlotFloats, full + s1);
+                bbox_load<AXIS>(itn, dn, nxt, buf + (size_t)s1 * kSlotFloats, full + s1);
+                ++nxt;
             }
         }
         if (!has_next) break;
         bulk_wait_read<0>();
-        if (B - 1 < Bn) {
+        if (nxt < Bn) {
             const int s0 = (int)perm_get(perm, 0);
-            bbox_load<AXIS>(itn, dn, B - 1, buf + (size_t)s0 * kSlotFloats, full + s0);
+            bbox_load<AXIS>(itn, dn, nxt, buf + (size_t)s0 * kSlotFloats, full + s0);
+            ++nxt;
         }
-        for (int j = B; j < Bn; ++j) {  // slots this tile left unused
-            const int sj = (int)perm_get(perm, j);
-            bbox_load<AXIS>(itn, dn, j, buf + (size_t)sj * kSlotFloats, full + sj);
-        }
-        perm = perm_next(perm, B);
+        perm = permn;
         t = tn;
         d = dn;
         item = itemn;
@@ -1014,7 +1026,7 @@ __global__ void __launch_bounds__(64 * kBatchWarps, 1) k_sweep_batch(const __gri
     if (warp >= W) {
         if (lane == 0 && t_begin < t_end)
             batch_producer<AXIS>(a, slots + (size_t)wi * Bmax * kSlotFloats, full + wi * kBatchMaxGroups,
-                                 empty + wi * kBatchMaxGroups, t_begin, t_end);
+                                 empty + wi * kBatchMaxGroups, t_begin, t_end, Bmax);
         return;
     }
     float* buf = slots + (size_t)warp * Bmax * kSlotFloats;
@@ -1038,7 +1050,7 @@ __global__ void __launch_bounds__(64 * kBatchWarps, 1) k_sweep_batch(const __gri
             staged = d.item;
         }
         if (!batch_tile<AXIS>(a, it, d, buf, fb, eb, sE, perm, fph)) break;
-        perm = perm_next(perm, it.B);
+        if (t + 1 < t_end) perm = batch_perm_next(perm, it.B, a.items[dnext.item].B, Bmax);
     }
 }
 
