@@ -569,7 +569,12 @@ def run_c4(args, rank, world, local_rank):
     stream = torch.cuda.Stream()
     sims, edges = c4_members(gb, stream)
     ens = gb.Ensemble(sims)
-    taken, branches, warps = ens.tune(SUBSTEPS)
+    if args.c4_form == "tuned":
+        taken, branches, warps = ens.tune(SUBSTEPS)
+    else:
+        taken, branches, warps = 0, 4, 0
+        ens.configure(branches, warps)
+        ens.set_batched(args.c4_form == "batched")
     batched = ens.batched()
     ens.run_mechanics(max(0, args.warmup - taken) + 2, SUBSTEPS)
     ens.sync()
@@ -628,7 +633,7 @@ def run_c4(args, rank, world, local_rank):
             "config": {"workload": C4_WORKLOAD, "members": C4_MEMBERS, "voxels_total": int((edges ** 3).sum()),
                        "cells_total_start": int(ncells0), "substeps_per_step": SUBSTEPS,
                        "biology_period_steps": C4_BIO, "tuned_branches": branches, "tuned_sweep_warps": warps,
-                       "tuned_batched_lod": batched,
+                       "tuned_batched_lod": batched, "form": args.c4_form,
                        "cells_cap": "each member's draw capped at 0.35 of its domain volume at packing 0.6, so the "
                                     "spheroid (radius 0.44 of the edge) fits its grid",
                        "tuning_steps": taken, "parallelism": "replicas"},
@@ -985,6 +990,8 @@ def main():
                          "against the plain solver at 256^3; lod: LOD substeps alone (--lod-n, --lod-subs)")
     ap.add_argument("--surrogate-weights", default=None, help="c5: weight file (default: the packaged one)")
     ap.add_argument("--no-conv-ring", action="store_true", help="c5: convolutions without the row ring")
+    ap.add_argument("--c4-form", choices=("tuned", "members", "batched"), default="tuned",
+                    help="c4: the tuner's choice, or 4 branches with LOD per member or batched over all members")
     ap.add_argument("--lod-n", type=int, default=400, help="lod: grid edge")
     ap.add_argument("--lod-subs", type=int, choices=(1, 2), default=2, help="lod: substrates")
     ap.add_argument("--no-extras", action="store_true",
