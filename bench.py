@@ -923,8 +923,15 @@ def run_reference(args, local_rank, world):
                        "voxel_updates_per_s_lod": N ** 3 * NSUB * SUBSTEPS * K / (t_lod / 1e3),
                        "ms_fm_update": t_fm / K, "ms_prelod": t_pre / K, "ms_lod_10_substeps": t_lod / K,
                        "lod_256cube_surrogate_workload": c5,
-                       "ms_per_step_each": {"min": float(np.min(per_step)), "median": float(np.median(per_step)),
-                                            "max": float(np.max(per_step))}},
+                       # every facade synchronises the device, so a step's time includes any host-side
+                       # pause between its launches; the spread shows how much of the mean that is
+                       "ms_per_step_each": {"min": float(np.min(per_step)),
+                                            "p10": float(np.percentile(per_step, 10)),
+                                            "median": float(np.median(per_step)),
+                                            "p90": float(np.percentile(per_step, 90)),
+                                            "max": float(np.max(per_step)),
+                                            "steps_over_twice_the_median":
+                                                int(np.sum(np.asarray(per_step) > 2 * np.median(per_step)))}},
         "e2e": {"value": cnt[1] / (t_e2e / 1e3), "unit": "cell-updates/s", "steps": ke,
                 "h2d_bytes_per_step": int(ncell * 72), "d2h_bytes_per_step": int(ncell * 72)},
         "clocks": sampler.summary(),
