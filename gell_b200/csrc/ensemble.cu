@@ -8,10 +8,12 @@
 // member's cell count, substrates or double-buffer assignment, or the substep count, changed.
 // gell_ensemble_tune times a few branch counts and sweep tile widths and keeps the fastest.
 //
-// Batched LOD (gell_ensemble_set_batched, or chosen by the tuner): each captured step is every
-// member's FM_update and PreLOD on the branches, then the LOD substeps of ALL members as one
-// launch per sweep axis (and one for the uptake source) over a device-side work list of every
-// member's line tiles (gell::lod_batch_run), instead of four launches per member and substep.
+// Batched (gell_ensemble_set_batched, or chosen by the tuner): each captured step is the FM_update
+// and PreLOD of ALL members as one launch per kernel (gell::mech_batch_step: keys, the sort's
+// passes, gather, force and move, the uptake map), then their LOD substeps as one launch per sweep
+// axis (and one for the uptake source) over a device-side work list of every member's line tiles
+// (gell::lod_batch_run), instead of per-member launches on the branches.  Ensembles beyond the
+// batched mechanics' limits (64 members, 4 substrates each) run their mechanics on the branches.
 #include <initializer_list>
 #include <vector>
 
@@ -78,7 +80,14 @@ gell_status capture(gell_ensemble* e, int substeps) {
     // all members' LOD substeps as one launch per sweep on the origin stream; otherwise each member's
     // two whole steps on its branch
     const int rounds = e->batched ? 2 : 1;
+    // batched: every member's FM_update and PreLOD as one launch per kernel too, when they fit
+    const bool mech_batched = e->batched && gell::mech_batch_ok(e->m);
     for (int r = 0; r < rounds && ce == cudaSuccess && st == GELL_OK; ++r) {
+        if (mech_batched) {
+            st = gell::mech_batch_step(e->m, e->origin);
+            if (st == GELL_OK) st = gell::lod_batch_run(e->batch, e->origin, substeps);
+            continue;
+        }
         ce = cudaEventRecord(e->fork, e->origin);
         for (int b = 0; b < nb && ce == cudaSuccess; ++b) ce = cudaStreamWaitEvent(e->pool[b], e->fork, 0);
         for (size_t i = 0; i < n && ce == cudaSuccess && st == GELL_OK; ++i) {

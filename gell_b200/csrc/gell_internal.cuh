@@ -279,6 +279,10 @@ gell_status lod_batch_build(const std::vector<gell_ctx*>& members, LodBatch** ou
 gell_status lod_batch_run(LodBatch* b, cudaStream_t st, int substeps);
 void lod_batch_free(LodBatch* b);
 gell_status prelod(gell_ctx* c, int sub);
+// FM_update and PreLOD of every member of an ensemble, one launch per kernel for all members, on
+// `st` (mech.cu); mech_batch_ok says whether the members fit its limits (64 members, 4 substrates)
+bool mech_batch_ok(const std::vector<gell_ctx*>& members);
+gell_status mech_batch_step(const std::vector<gell_ctx*>& members, cudaStream_t st);
 gell_status fm_update(gell_ctx* c);
 gell_status selftest_timeout(gell_ctx* c, int polls);
 // one mechanics step (fm_update, prelod of all substrates, `substeps` LOD substeps) on c->stream

@@ -34,6 +34,7 @@
 
 #include "async_copy.cuh"
 #include "gell_internal.cuh"
+#include "mech_body.cuh"
 
 namespace gell {
 
@@ -1163,47 +1164,9 @@ struct PreArgs {
     float dead;
 };
 
-// Clear the lines flagged by the previous map (oxy_consumption_reset, include/LODkernel.cuh:183-190,
-// restricted to the lines that can be nonzero).
-// One warp per listed line: the row (P floats, P a multiple of 4) is cleared with 16-byte stores.
-__global__ void k_rate_reset(PreArgs a) {
-    const int P4 = a.g.P >> 2;
-    const int lane = threadIdx.x & 31;
-    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int s = 0; s < a.nsub; ++s) {
-        const int cnt = *a.count[s];
-        for (long long li = gw; li < cnt; li += nw) {
-            const int line = a.list[s][li];
-            float4* row = reinterpret_cast<float4*>(a.rate[s] + (long long)line * a.g.P);
-            for (int x4 = lane; x4 < P4; x4 += 32) row[x4] = z;
-            if (lane == 0) a.flag[s][line] = 0;
-        }
-    }
-}
+__global__ void k_rate_reset(PreArgs a) { rate_reset_body(a, blockIdx.x, gridDim.x); }
 
-// oxy_consumption_update (include/LODkernel.cuh:12-22) with Cell::O2_consume (include/Cells.cuh:74-89)
-// at O2 = 1: rate[mesh_idx] += coef * (V/len/len/len) (times the dead factor for phase >= 3).
-__global__ void k_rate_accum(CellsSoA c, int n, PreArgs a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || !c.sign[i]) return;
-    const int ph = c.phase[i];
-    if (ph < 0) return;
-    const int N = a.g.N;
-    const int m = c.mesh[i];
-    if (m < 0 || (long long)m >= (long long)N * N * N) return;
-    const int x = m % N, line = m / N;
-    const float len = a.g.len;
-    const float vf = __fdiv_rn(__fdiv_rn(__fdiv_rn(c.V[i], len), len), len);
-    for (int s = 0; s < a.nsub; ++s) {
-        float r = __fmul_rn(a.coef[s], vf);
-        if (ph >= 3) r = __fmul_rn(r, a.dead);
-        atomicAdd(a.rate[s] + (long long)line * a.g.P + x, r);
-        uint32_t* f = a.flag[s] + line;
-        if (*(volatile uint32_t*)f == 0 && atomicExch(f, 1u) == 0u) a.list[s][atomicAdd(a.count[s], 1)] = line;
-    }
-}
+__global__ void k_rate_accum(CellsSoA c, int n, PreArgs a) { rate_accum_body(c, n, a, blockIdx.x); }
 
 int g_num_sms = 0;
 int num_sms() {

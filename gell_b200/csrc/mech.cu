@@ -9,158 +9,23 @@
 //   k_force_move  forcekernel (:56-118) and movementkernel (:130-158) fused: one thread per cell
 //                 walks the 27 bins in the reference's order and applies the move; it reads the
 //                 sorted buffer and writes the other one, so no cell sees a moved neighbour
-#include "gell_internal.cuh"
+#include "mech_body.cuh"
 
 namespace gell {
 
 namespace {
 
-// Also advances the cell-list epoch, which lives in device memory so that a captured step reads
-// the current one when it is replayed.
 __global__ void k_keys(CellsSoA c, int n, Geom g, uint32_t* __restrict__ keys, int* __restrict__ epoch) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) *epoch += 1;
-    if (i >= n) return;
-    const float4 pr = c.posr[i];
-    const int3 b = find_bin(pr.x, pr.y, pr.z, g.len);
-    if (!inside(b.x, b.y, b.z, g.N)) {
-        c.sign[i] = 0;
-        keys[i] = 0u;
-        return;
-    }
-    keys[i] = morton3(b.x, b.y, b.z) + 1u;
-    c.mesh[i] = b.x + b.y * g.N + b.z * g.N * g.N;
+    keys_body(c, n, g, keys, epoch, blockIdx.x);
 }
 
 __global__ void k_gather(CellsSoA s, CellsSoA d, const uint32_t* __restrict__ keys,
                          const uint32_t* __restrict__ perm, int n, int4* __restrict__ bins,
                          const int* __restrict__ epoch_p) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int epoch = *epoch_p;
-    const int j = (int)perm[i];
-    d.sign[i] = s.sign[j];
-    const int m = s.mesh[j];
-    d.mesh[i] = m;
-    d.posr[i] = s.posr[j];
-    d.force[i] = s.force[j];
-    d.oldf[i] = s.oldf[j];
-    d.V[i] = s.V[j];
-    d.Vf[i] = s.Vf[j];
-    d.Vcs[i] = s.Vcs[j];
-    d.Vns[i] = s.Vns[j];
-    d.clock[i] = s.clock[j];
-    d.phase[i] = s.phase[j];
-    const uint32_t k = keys[i];
-    if (k == 0u) return;  // outside the grid: in no bin
-    // a run of equal keys is one bin; its head writes the start and epoch, its tail the end
-    if (i == 0 || keys[i - 1] != k) {
-        bins[m].x = i;
-        bins[m].z = epoch;
-    }
-    if (i == n - 1 || keys[i + 1] != k) bins[m].y = i;
+    gather_body(s, d, keys, perm, n, bins, epoch_p, blockIdx.x);
 }
 
-struct MechArgs {
-    CellsSoA cur, alt;
-    const int4* bins;
-    const int* epoch;
-    int n;
-    Geom g;
-    float max_dist, cccr, ccca;
-    double ra_ratio;
-    float half_dt;
-};
-
-// forcekernel + movementkernel.  Per candidate j, in the order xi, yi, zi (bins), then ascending
-// sorted index, with the cutoff `thres` carried from the previous accepted candidate:
-//   d = sqrt(float(double(fma(dz,dz, fma(dx,dx, dy*dy))) + 0.0001)); skip if d >= thres;
-//   R = max(r_j + r_i, 0.01); thres = float(double(R) * Ra_ratio); skip if d >= thres;
-//   coefr = Cccr*((1-d/R)^2/d) if d <= R; coefa = Ccca*((1-d/thres)^2/d);
-//   f = fma(p_i - p_j, coefr - coefa, f)
-// then pos += dt/2 * (3f - f_old) as fma(dt/2, fma(3, f, -f_old), pos).
-__global__ void __launch_bounds__(256) k_force_move(MechArgs a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
-    const uint8_t sg = a.cur.sign[i];
-    const float4 pr = a.cur.posr[i];
-    const float4 of = a.cur.oldf[i];
-    if (!sg) {
-        a.alt.sign[i] = 0;
-        a.alt.posr[i] = pr;
-        a.alt.oldf[i] = of;
-        a.alt.force[i] = a.cur.force[i];
-        a.alt.mesh[i] = a.cur.mesh[i];
-        return;
-    }
-    const int N = a.g.N;
-    const long long NN = (long long)N * N;
-    const int epoch = *a.epoch;
-    const int3 b = find_bin(pr.x, pr.y, pr.z, a.g.len);
-    float fx = 0.f, fy = 0.f, fz = 0.f;
-    float thres = a.max_dist;
-    // d >= thres is certain when |dp|^2 alone exceeds thres^2 (1 + 2^-20), a relative margin far
-    // above the roundings between |dp|^2 + 0.0001 and d: such candidates skip the double-precision
-    // add and the square root.  The float threshold is that bound rounded up.
-    float thr_hi = __double2float_ru((double)thres * (double)thres * (1.0 + 0x1p-20));
-    // the 27 bins in the reference's order: xi outer, then yi, then zi
-#pragma unroll 1
-    for (int o = 0; o < 27; ++o) {
-        const int xi = b.x - 1 + o / 9, yi = b.y - 1 + (o / 3) % 3, zi = b.z - 1 + o % 3;
-        if (!inside(xi, yi, zi, N)) continue;
-        const int4 e = a.bins[xi + (long long)yi * N + zi * NN];
-        if (e.z != epoch) continue;
-#pragma unroll 1
-        for (int j = e.x; j <= e.y; ++j) {
-            if (!a.cur.sign[j]) continue;
-            const float4 q = a.cur.posr[j];
-            const float dx = __fsub_rn(pr.x, q.x);
-            const float dy = __fsub_rn(pr.y, q.y);
-            const float dz = __fsub_rn(pr.z, q.z);
-            const float ss = __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
-            if (ss > thr_hi) continue;
-            const float d = __fsqrt_rn(__double2float_rn(__dadd_rn((double)ss, 0.0001)));
-            if (d >= thres) continue;
-            const float rs = __fadd_rn(q.w, pr.w);
-            const float R = rs > 0.01f ? rs : 0.01f;
-            thres = __double2float_rn(__dmul_rn((double)R, a.ra_ratio));
-            thr_hi = __double2float_ru((double)thres * (double)thres * (1.0 + 0x1p-20));
-            if (d >= thres) continue;
-            float cr = 0.f, ca = 0.f;
-            if (d <= R) {
-                const float t = __fsub_rn(1.f, __fdiv_rn(d, R));
-                cr = __fmul_rn(a.cccr, __fdiv_rn(__fmul_rn(t, t), d));
-            }
-            if (d <= thres) {
-                const float t = __fsub_rn(1.f, __fdiv_rn(d, thres));
-                ca = __fmul_rn(a.ccca, __fdiv_rn(__fmul_rn(t, t), d));
-            }
-            const float cf = __fsub_rn(cr, ca);
-            fx = __fmaf_rn(dx, cf, fx);
-            fy = __fmaf_rn(dy, cf, fy);
-            fz = __fmaf_rn(dz, cf, fz);
-        }
-    }
-    const float h = a.half_dt;
-    const float nx = __fmaf_rn(h, __fmaf_rn(3.f, fx, -of.x), pr.x);
-    const float ny = __fmaf_rn(h, __fmaf_rn(3.f, fy, -of.y), pr.y);
-    const float nz = __fmaf_rn(h, __fmaf_rn(3.f, fz, -of.z), pr.z);
-    const int3 nb = find_bin(nx, ny, nz, a.g.len);
-    if (!inside(nb.x, nb.y, nb.z, N)) {
-        // leaves the grid: only the sign changes (the reference returns before writing)
-        a.alt.sign[i] = 0;
-        a.alt.posr[i] = pr;
-        a.alt.oldf[i] = of;
-        a.alt.force[i] = make_float4(fx, fy, fz, 0.f);
-        a.alt.mesh[i] = a.cur.mesh[i];
-        return;
-    }
-    a.alt.sign[i] = 1;
-    a.alt.posr[i] = make_float4(nx, ny, nz, pr.w);
-    a.alt.oldf[i] = make_float4(fx, fy, fz, 0.f);
-    a.alt.force[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    a.alt.mesh[i] = nb.x + nb.y * N + nb.z * N * N;
-}
+__global__ void __launch_bounds__(256) k_force_move(MechArgs a) { force_move_body(a, blockIdx.x); }
 
 // Reference-shaped s/e arrays (first and last LIVE sorted index per bin, Max_Cell_num+1 / -1 when
 // empty) rebuilt from the cell list, for the parity tests.
@@ -224,6 +89,303 @@ gell_status fm_update(gell_ctx* c) {
     }
     c->sorted_valid = true;
     c->rate_valid = false;
+    return GELL_OK;
+}
+
+// ------------------------------------------------------------------ ensembles: batched mechanics
+//
+// One FM_update and one PreLOD of every member of an ensemble as one launch per kernel: keys, the
+// sort's three kernels per digit pass, the gather, the force and move, the uptake map.  A batched
+// launch's blocks are the members' own blocks laid end to end; block b runs the kernel body (the
+// same device code as the member's own launch, mech_body.cuh) for block b - start[m] of the member
+// m whose range holds b.  The arguments travel by value in the launch (at most kBatchMembers
+// members), so a captured graph holds them and no device table is kept.  Members keep their own
+// digit widths and pass counts (their grids differ); a member with fewer passes sits out the last
+// ones.  The host swaps each member's buffers exactly as fm_update and prelod do.
+
+namespace {
+
+constexpr int kBatchMembers = 64;
+constexpr int kBatchSub = 4;
+
+struct BlockMap {
+    int nm;
+    int start[kBatchMembers + 1];  // member m owns blocks [start[m], start[m+1])
+};
+
+// member of block b (binary search over the starts) and the block's index inside the member
+__device__ __forceinline__ int member_of(const BlockMap& bm, int b, int& local) {
+    int lo = 0, hi = bm.nm;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (bm.start[mid] <= b) lo = mid;
+        else hi = mid;
+    }
+    local = b - bm.start[lo];
+    return lo;
+}
+
+struct KeysJob {
+    CellsSoA c;
+    uint32_t* keys;
+    int* epoch;
+    Geom g;
+    int n;
+};
+struct KeysBatch {
+    BlockMap map;
+    KeysJob job[kBatchMembers];
+};
+__global__ void k_keys_batch(const __grid_constant__ KeysBatch b) {
+    int local;
+    const KeysJob& j = b.job[member_of(b.map, blockIdx.x, local)];
+    keys_body(j.c, j.n, j.g, j.keys, j.epoch, local);
+}
+
+struct SortJob {
+    const uint32_t* kin;
+    const uint32_t* vin;
+    uint32_t* kout;
+    uint32_t* vout;
+    uint32_t* hist;
+    int n, nb, shift, R, iota;
+};
+struct SortBatch {
+    BlockMap tiles, digits;
+    SortJob job[kBatchMembers];
+};
+__global__ void __launch_bounds__(kSortThreads) k_hist_batch(const __grid_constant__ SortBatch b) {
+    int local;
+    const SortJob& j = b.job[member_of(b.tiles, blockIdx.x, local)];
+    hist_body(j.kin, j.n, j.shift, j.R, j.hist, j.nb, local);
+}
+__global__ void __launch_bounds__(kSortThreads) k_digit_scan_batch(const __grid_constant__ SortBatch b) {
+    int local;
+    const SortJob& j = b.job[member_of(b.digits, blockIdx.x, local)];
+    digit_scan_body(j.hist, j.nb, j.hist + (size_t)j.R * j.nb, local);
+}
+__global__ void __launch_bounds__(kSortThreads) k_scatter_batch(const __grid_constant__ SortBatch b) {
+    int local;
+    const SortJob& j = b.job[member_of(b.tiles, blockIdx.x, local)];
+    scatter_body(j.kin, j.vin, j.kout, j.vout, j.n, j.shift, j.R, j.hist, j.nb, j.hist + (size_t)j.R * j.nb, j.iota,
+                 local);
+}
+
+struct GatherJob {
+    CellsSoA s, d;
+    const uint32_t* keys;
+    const uint32_t* perm;
+    int4* bins;
+    const int* epoch;
+    int n;
+};
+struct GatherBatch {
+    BlockMap map;
+    GatherJob job[kBatchMembers];
+};
+__global__ void k_gather_batch(const __grid_constant__ GatherBatch b) {
+    int local;
+    const GatherJob& j = b.job[member_of(b.map, blockIdx.x, local)];
+    gather_body(j.s, j.d, j.keys, j.perm, j.n, j.bins, j.epoch, local);
+}
+
+struct ForceBatch {
+    BlockMap map;
+    MechArgs job[kBatchMembers];
+};
+__global__ void __launch_bounds__(256) k_force_move_batch(const __grid_constant__ ForceBatch b) {
+    int local;
+    const MechArgs& j = b.job[member_of(b.map, blockIdx.x, local)];
+    force_move_body(j, local);
+}
+
+// the uptake map's arguments (lod.cu's PreArgs for at most kBatchSub substrates) and the cells
+struct PreJob {
+    float* rate[kBatchSub];
+    uint32_t* flag[kBatchSub];
+    int* list[kBatchSub];
+    int* count[kBatchSub];
+    float coef[kBatchSub];
+    CellsSoA c;
+    Geom g;
+    float dead;
+    int nsub;
+    int n;
+};
+struct PreBatch {
+    BlockMap map;  // k_rate_accum blocks
+    PreJob job[kBatchMembers];
+};
+constexpr int kResetBlocks = 8;  // k_rate_reset blocks per member (a grid-stride loop over its listed lines)
+__global__ void k_rate_reset_batch(const __grid_constant__ PreBatch b) {
+    rate_reset_body(b.job[blockIdx.y], blockIdx.x, gridDim.x);
+}
+__global__ void k_zero_counts_batch(const __grid_constant__ PreBatch b) {
+    const int m = threadIdx.x / kBatchSub, s = threadIdx.x % kBatchSub;
+    if (m < b.map.nm && s < b.job[m].nsub) *b.job[m].count[s] = 0;
+}
+__global__ void k_rate_accum_batch(const __grid_constant__ PreBatch b) {
+    int local;
+    const PreJob& j = b.job[member_of(b.map, blockIdx.x, local)];
+    rate_accum_body(j.c, j.n, j, local);
+}
+
+static_assert(sizeof(KeysBatch) <= 32000 && sizeof(SortBatch) <= 32000 && sizeof(GatherBatch) <= 32000 &&
+                  sizeof(ForceBatch) <= 32000 && sizeof(PreBatch) <= 32000,
+              "batched arguments exceed the kernel parameter limit");
+static_assert(kBatchMembers * kBatchSub <= 256, "k_zero_counts_batch runs one thread per (member, substrate)");
+
+// start[] of a map over blocks[i] blocks per entry; total blocks
+int fill_map(BlockMap& m, const std::vector<int>& blocks) {
+    m.nm = (int)blocks.size();
+    int t = 0;
+    for (size_t i = 0; i < blocks.size(); ++i) {
+        m.start[i] = t;
+        t += blocks[i];
+    }
+    m.start[blocks.size()] = t;
+    return t;
+}
+
+}  // namespace
+
+bool mech_batch_ok(const std::vector<gell_ctx*>& ms) {
+    if (ms.empty() || ms.size() > (size_t)kBatchMembers) return false;
+    for (const gell_ctx* c : ms)
+        if (c->subs.size() > (size_t)kBatchSub) return false;
+    return true;
+}
+
+gell_status mech_batch_step(const std::vector<gell_ctx*>& ms, cudaStream_t st) {
+    if (!mech_batch_ok(ms)) return GELL_ERR_UNSUPPORTED;
+    gell_ctx* c0 = ms[0];  // the batched launches are counted (and profiled) on the first member
+
+    // FM_update of the members that hold cells
+    std::vector<gell_ctx*> fm;
+    for (gell_ctx* c : ms)
+        if (c->n > 0) fm.push_back(c);
+    if (!fm.empty()) {
+        const int nf = (int)fm.size();
+        std::vector<int> blocks(nf);
+        for (int i = 0; i < nf; ++i) blocks[i] = blocks_for(fm[i]->n, 256);
+
+        KeysBatch kb{};
+        const int kblocks = fill_map(kb.map, blocks);
+        for (int i = 0; i < nf; ++i) {
+            gell_ctx* c = fm[i];
+            kb.job[i] = KeysJob{c->cur(), c->sort.keys[0], c->dev_epoch, c->g, c->n};
+        }
+        GELL_KERNEL(c0, "k_keys_batch", k_keys_batch<<<kblocks, 256, 0, st>>>(kb));
+
+        // the sort: each member's own digit width and pass count (radix_sort's rule)
+        std::vector<int> passes(nf), dbits(nf), in(nf, 0), iota(nf, 1);
+        int maxp = 0;
+        for (int i = 0; i < nf; ++i) {
+            const int bits = key_bits(fm[i]->g.N);
+            passes[i] = (bits + 7) / 8 < 1 ? 1 : (bits + 7) / 8;
+            dbits[i] = (bits + passes[i] - 1) / passes[i];
+            maxp = passes[i] > maxp ? passes[i] : maxp;
+        }
+        for (int p = 0; p < maxp; ++p) {
+            SortBatch sb{};
+            std::vector<int> tiles, digits, who;
+            for (int i = 0; i < nf; ++i) {
+                if (p >= passes[i]) continue;
+                gell_ctx* c = fm[i];
+                SortScratch& S = c->sort;
+                const int nb = (c->n + kSortTile - 1) / kSortTile;
+                const int R = 1 << dbits[i];
+                sb.job[who.size()] = SortJob{S.keys[in[i]], S.vals[in[i]], S.keys[in[i] ^ 1], S.vals[in[i] ^ 1], S.hist,
+                                             c->n, nb, p * dbits[i], R, iota[i]};
+                tiles.push_back(nb);
+                digits.push_back(R);
+                who.push_back(i);
+            }
+            const int ntiles = fill_map(sb.tiles, tiles);
+            const int ndigits = fill_map(sb.digits, digits);
+            GELL_KERNEL(c0, "k_hist_batch", k_hist_batch<<<ntiles, kSortThreads, 0, st>>>(sb));
+            GELL_KERNEL(c0, "k_digit_scan_batch", k_digit_scan_batch<<<ndigits, kSortThreads, 0, st>>>(sb));
+            GELL_KERNEL(c0, "k_scatter_batch", k_scatter_batch<<<ntiles, kSortThreads, 0, st>>>(sb));
+            for (int i : who) {
+                in[i] ^= 1;
+                iota[i] = 0;
+            }
+        }
+
+        GatherBatch gb{};
+        const int gblocks = fill_map(gb.map, blocks);
+        for (int i = 0; i < nf; ++i) {
+            gell_ctx* c = fm[i];
+            c->sort.which = in[i];
+            gb.job[i] = GatherJob{c->cur(), c->alt(), c->sort.keys[in[i]], c->sort.vals[in[i]], c->bins, c->dev_epoch,
+                                  c->n};
+            c->swap_all();
+        }
+        GELL_KERNEL(c0, "k_gather_batch", k_gather_batch<<<gblocks, 256, 0, st>>>(gb));
+
+        ForceBatch fb{};
+        const int fblocks = fill_map(fb.map, blocks);
+        for (int i = 0; i < nf; ++i) {
+            gell_ctx* c = fm[i];
+            MechArgs& a = fb.job[i];
+            a.cur = c->cur();
+            a.alt = c->alt();
+            a.bins = c->bins;
+            a.epoch = c->dev_epoch;
+            a.n = c->n;
+            a.g = c->g;
+            a.max_dist = c->P.cc_max_dist;
+            a.cccr = c->P.cccr;
+            a.ccca = c->P.ccca;
+            a.ra_ratio = c->P.ra_ratio;
+            a.half_dt = c->P.mechanics_dt / 2.f;
+            c->sign.swap();
+            c->mesh.swap();
+            c->posr.swap();
+            c->force.swap();
+            c->oldf.swap();
+        }
+        GELL_KERNEL(c0, "k_force_move_batch", k_force_move_batch<<<fblocks, 256, 0, st>>>(fb));
+    }
+    for (gell_ctx* c : ms) {
+        c->sorted_valid = true;
+        c->rate_valid = false;
+    }
+
+    // PreLOD of every member with substrates: clear the lines of the last map, reset the line
+    // counts, accumulate the new map
+    std::vector<gell_ctx*> pm;
+    for (gell_ctx* c : ms)
+        if (!c->subs.empty()) pm.push_back(c);
+    if (!pm.empty()) {
+        PreBatch pb{};
+        std::vector<int> blocks;
+        for (size_t i = 0; i < pm.size(); ++i) {
+            gell_ctx* c = pm[i];
+            PreJob& j = pb.job[i];
+            for (size_t s = 0; s < c->subs.size(); ++s) {
+                Substrate& S = c->subs[s];
+                j.rate[s] = S.rate;
+                j.flag[s] = S.line_flag;
+                j.list[s] = S.line_list;
+                j.count[s] = S.line_count;
+                j.coef[s] = S.s.uptake;
+            }
+            j.nsub = (int)c->subs.size();
+            j.c = c->cur();
+            j.g = c->g;
+            j.dead = c->P.dead_uptake_factor;
+            j.n = c->n;
+            // a member without cells launches no k_rate_accum block
+            blocks.push_back(c->n > 0 ? blocks_for(c->n, 256) : 0);
+        }
+        const int ablocks = fill_map(pb.map, blocks);
+        GELL_KERNEL(c0, "k_rate_reset_batch",
+                    k_rate_reset_batch<<<dim3(kResetBlocks, (unsigned)pm.size()), 256, 0, st>>>(pb));
+        GELL_KERNEL(c0, "k_zero_counts_batch", k_zero_counts_batch<<<1, 256, 0, st>>>(pb));
+        if (ablocks > 0) GELL_KERNEL(c0, "k_rate_accum_batch", k_rate_accum_batch<<<ablocks, 256, 0, st>>>(pb));
+        for (gell_ctx* c : pm) c->rate_valid = true;
+    }
     return GELL_OK;
 }
 

@@ -11,36 +11,14 @@
 // then scatter).  A tile is 8 warps x 16 items; item k of lane l of warp w is tile element
 // w*512 + k*32 + l, so processing k in order and lanes in order visits the tile in input order,
 // which is what makes the ranks, and the sort, stable.
-#include "gell_internal.cuh"
+#include "mech_body.cuh"
 
 namespace gell {
 
 namespace {
-constexpr int kThreads = 256;
-constexpr int kItems = 16;
-constexpr int kTile = kThreads * kItems;  // 4096
-constexpr unsigned FULL = 0xffffffffu;
-
-__device__ __forceinline__ unsigned lanemask_lt() {
-    unsigned m;
-    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-    return m;
-}
-
-__global__ void __launch_bounds__(kThreads) k_hist(const uint32_t* __restrict__ keys, int n, int shift,
+__global__ void __launch_bounds__(kSortThreads) k_hist(const uint32_t* __restrict__ keys, int n, int shift,
                                                    int R, uint32_t* __restrict__ hist, int nb) {
-    __shared__ uint32_t h[256];
-    for (int d = threadIdx.x; d < R; d += kThreads) h[d] = 0;
-    __syncthreads();
-    const long long base = (long long)blockIdx.x * kTile;
-    const uint32_t mask = (uint32_t)R - 1u;
-#pragma unroll 4
-    for (int k = 0; k < kItems; ++k) {
-        long long i = base + k * kThreads + threadIdx.x;
-        if (i < n) atomicAdd(&h[(keys[i] >> shift) & mask], 1u);
-    }
-    __syncthreads();
-    for (int d = threadIdx.x; d < R; d += kThreads) hist[(long long)d * nb + blockIdx.x] = h[d];
+    hist_body(keys, n, shift, R, hist, nb, blockIdx.x);
 }
 
 // Exclusive scan of m entries in place by one CTA of 1024 threads; total to *total if not null.
@@ -80,118 +58,26 @@ __global__ void __launch_bounds__(1024) k_scan_single(uint32_t* a, long long m, 
     if (total && t == 1023) *total = (int)(warp_sums[31]);
 }
 
-// Exclusive scan of one digit's per-tile counts (row d of the digit-major table), in place, by
-// CTA d; the digit's total goes to totals[d].  The scatter adds the prefix of the totals.
-__global__ void __launch_bounds__(kThreads) k_digit_scan(uint32_t* __restrict__ hist, int nb,
+__global__ void __launch_bounds__(kSortThreads) k_digit_scan(uint32_t* __restrict__ hist, int nb,
                                                          uint32_t* __restrict__ totals) {
-    __shared__ uint32_t ws[kThreads / 32];
-    uint32_t* row = hist + (long long)blockIdx.x * nb;
-    const int per = (nb + kThreads - 1) / kThreads;
-    const int lo = threadIdx.x * per, hi = lo + per < nb ? lo + per : nb;
-    uint32_t s = 0;
-    for (int i = lo; i < hi; ++i) s += row[i];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    uint32_t x = s;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(FULL, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) ws[w] = x;
-    __syncthreads();
-    uint32_t wpre = 0;
-    for (int j = 0; j < w; ++j) wpre += ws[j];
-    uint32_t run = wpre + x - s;
-    for (int i = lo; i < hi; ++i) {
-        const uint32_t v = row[i];
-        row[i] = run;
-        run += v;
-    }
-    if (threadIdx.x == kThreads - 1) totals[blockIdx.x] = run;
+    digit_scan_body(hist, nb, totals, blockIdx.x);
 }
 
-__global__ void __launch_bounds__(kThreads) k_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+__global__ void __launch_bounds__(kSortThreads) k_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                                                       uint32_t* __restrict__ kout, uint32_t* __restrict__ vout, int n,
                                                       int shift, int R, const uint32_t* __restrict__ offs, int nb,
                                                       const uint32_t* __restrict__ totals, int iota) {
-    __shared__ uint32_t wcnt[kThreads / 32][256];
-    __shared__ uint32_t gbase[256];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int i = threadIdx.x; i < (kThreads / 32) * 256; i += kThreads) (&wcnt[0][0])[i] = 0;
-    if (w == 0) {
-        // exclusive prefix of the digit totals: lane l sums digits 8l .. 8l+7 (R <= 256)
-        uint32_t t[8], s = 0;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const int d = 8 * lane + k;
-            t[k] = d < R ? totals[d] : 0u;
-            s += t[k];
-        }
-        uint32_t x = s;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(FULL, x, o);
-            if (lane >= o) x += y;
-        }
-        uint32_t run = x - s;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const int d = 8 * lane + k;
-            if (d < R) gbase[d] = run;
-            run += t[k];
-        }
-    }
-    __syncthreads();
-    for (int d = threadIdx.x; d < R; d += kThreads) gbase[d] += offs[(long long)d * nb + blockIdx.x];
-    __syncthreads();
-    const uint32_t mask = (uint32_t)R - 1u;
-    const long long base = (long long)blockIdx.x * kTile + w * (kTile / (kThreads / 32));
-    uint32_t key[kItems], loc[kItems];
-    const unsigned lt = lanemask_lt();
-#pragma unroll
-    for (int k = 0; k < kItems; ++k) {
-        const long long i = base + k * 32 + lane;
-        const bool valid = i < n;
-        key[k] = valid ? kin[i] : 0u;
-        const uint32_t dig = (key[k] >> shift) & mask;
-        const unsigned peers = __match_any_sync(FULL, valid ? dig : 0xffffffffu);
-        const uint32_t before = wcnt[w][dig & 255];
-        loc[k] = before + __popc(peers & lt);
-        __syncwarp();
-        if (valid && (peers & lt) == 0) wcnt[w][dig] = before + __popc(peers);
-        __syncwarp();
-    }
-    __syncthreads();
-    for (int d = threadIdx.x; d < R; d += kThreads) {
-        uint32_t run = 0;
-#pragma unroll
-        for (int ww = 0; ww < kThreads / 32; ++ww) {
-            uint32_t c = wcnt[ww][d];
-            wcnt[ww][d] = run;
-            run += c;
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < kItems; ++k) {
-        const long long i = base + k * 32 + lane;
-        if (i < n) {
-            const uint32_t dig = (key[k] >> shift) & mask;
-            const uint32_t pos = gbase[dig] + wcnt[w][dig] + loc[k];
-            kout[pos] = key[k];
-            vout[pos] = iota ? (uint32_t)i : vin[i];
-        }
-    }
+    scatter_body(kin, vin, kout, vout, n, shift, R, offs, nb, totals, iota, blockIdx.x);
 }
 
 // Scan helpers: per-tile sums, then tile-local exclusive scan plus the tile's offset.
-__global__ void __launch_bounds__(kThreads) k_tile_sum(const uint32_t* __restrict__ in, int n, uint32_t* __restrict__ sums) {
-    __shared__ uint32_t ws[kThreads / 32];
-    const long long base = (long long)blockIdx.x * kTile;
+__global__ void __launch_bounds__(kSortThreads) k_tile_sum(const uint32_t* __restrict__ in, int n, uint32_t* __restrict__ sums) {
+    __shared__ uint32_t ws[kSortThreads / 32];
+    const long long base = (long long)blockIdx.x * kSortTile;
     uint32_t s = 0;
 #pragma unroll 4
-    for (int k = 0; k < kItems; ++k) {
-        long long i = base + k * kThreads + threadIdx.x;
+    for (int k = 0; k < kSortItems; ++k) {
+        long long i = base + k * kSortThreads + threadIdx.x;
         if (i < n) s += in[i];
     }
 #pragma unroll
@@ -200,21 +86,21 @@ __global__ void __launch_bounds__(kThreads) k_tile_sum(const uint32_t* __restric
     __syncthreads();
     if (threadIdx.x == 0) {
         uint32_t t = 0;
-        for (int w = 0; w < kThreads / 32; ++w) t += ws[w];
+        for (int w = 0; w < kSortThreads / 32; ++w) t += ws[w];
         sums[blockIdx.x] = t;
     }
 }
 
-__global__ void __launch_bounds__(kThreads) k_tile_scan(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, int n,
+__global__ void __launch_bounds__(kSortThreads) k_tile_scan(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, int n,
                                                         const uint32_t* __restrict__ offs) {
     // thread t owns elements base + t*16 .. +15 (contiguous), so a thread-serial scan inside
     // plus a block scan over threads gives the tile's exclusive scan in order
-    __shared__ uint32_t ws[kThreads / 32];
-    const long long base = (long long)blockIdx.x * kTile + (long long)threadIdx.x * kItems;
-    uint32_t v[kItems];
+    __shared__ uint32_t ws[kSortThreads / 32];
+    const long long base = (long long)blockIdx.x * kSortTile + (long long)threadIdx.x * kSortItems;
+    uint32_t v[kSortItems];
     uint32_t s = 0;
 #pragma unroll
-    for (int k = 0; k < kItems; ++k) {
+    for (int k = 0; k < kSortItems; ++k) {
         long long i = base + k;
         v[k] = i < n ? in[i] : 0u;
         s += v[k];
@@ -232,7 +118,7 @@ __global__ void __launch_bounds__(kThreads) k_tile_scan(const uint32_t* __restri
     for (int j = 0; j < w; ++j) wpre += ws[j];
     uint32_t run = offs[blockIdx.x] + wpre + x - s;
 #pragma unroll
-    for (int k = 0; k < kItems; ++k) {
+    for (int k = 0; k < kSortItems; ++k) {
         long long i = base + k;
         if (i < n) out[i] = run;
         run += v[k];
@@ -242,7 +128,7 @@ __global__ void __launch_bounds__(kThreads) k_tile_scan(const uint32_t* __restri
 }  // namespace
 
 // digit-major count table, then the 256 digit totals
-size_t sort_hist_entries(int cap) { return (size_t)256 * ((cap + kTile - 1) / kTile) + 256 + 64; }
+size_t sort_hist_entries(int cap) { return (size_t)256 * ((cap + kSortTile - 1) / kSortTile) + 256 + 64; }
 
 gell_status radix_sort(gell_ctx* c, int n, int bits, bool vals_are_iota) {
     SortScratch& S = c->sort;
@@ -251,7 +137,7 @@ gell_status radix_sort(gell_ctx* c, int n, int bits, bool vals_are_iota) {
         S.which = 0;
         return GELL_OK;
     }
-    const int nb = (n + kTile - 1) / kTile;
+    const int nb = (n + kSortTile - 1) / kSortTile;
     int passes = (bits + 7) / 8;
     if (passes < 1) passes = 1;
     const int d = (bits + passes - 1) / passes;
@@ -259,10 +145,10 @@ gell_status radix_sort(gell_ctx* c, int n, int bits, bool vals_are_iota) {
     bool iota = vals_are_iota;
     for (int p = 0; p < passes; ++p) {
         const int shift = p * d;
-        GELL_KERNEL(c, "k_hist", k_hist<<<nb, kThreads, 0, c->stream>>>(S.keys[in], n, shift, R, S.hist, nb));
+        GELL_KERNEL(c, "k_hist", k_hist<<<nb, kSortThreads, 0, c->stream>>>(S.keys[in], n, shift, R, S.hist, nb));
         uint32_t* totals = S.hist + (size_t)R * nb;
-        GELL_KERNEL(c, "k_digit_scan", k_digit_scan<<<R, kThreads, 0, c->stream>>>(S.hist, nb, totals));
-        GELL_KERNEL(c, "k_scatter", k_scatter<<<nb, kThreads, 0, c->stream>>>(S.keys[in], S.vals[in], S.keys[in ^ 1], S.vals[in ^ 1], n, shift,
+        GELL_KERNEL(c, "k_digit_scan", k_digit_scan<<<R, kSortThreads, 0, c->stream>>>(S.hist, nb, totals));
+        GELL_KERNEL(c, "k_scatter", k_scatter<<<nb, kSortThreads, 0, c->stream>>>(S.keys[in], S.vals[in], S.keys[in ^ 1], S.vals[in ^ 1], n, shift,
                                                    R, S.hist, nb, totals, iota ? 1 : 0));
         iota = false;
         in ^= 1;
@@ -276,10 +162,10 @@ gell_status scan_u32(gell_ctx* c, const uint32_t* in, uint32_t* out, int n, int*
         GELL_CUDA(c, cudaMemsetAsync(total_dev, 0, 4, c->stream));
         return GELL_OK;
     }
-    const int nb = (n + kTile - 1) / kTile;
-    GELL_KERNEL(c, "k_tile_sum", k_tile_sum<<<nb, kThreads, 0, c->stream>>>(in, n, c->scan_tmp));
+    const int nb = (n + kSortTile - 1) / kSortTile;
+    GELL_KERNEL(c, "k_tile_sum", k_tile_sum<<<nb, kSortThreads, 0, c->stream>>>(in, n, c->scan_tmp));
     GELL_KERNEL(c, "k_scan_single", k_scan_single<<<1, 1024, 0, c->stream>>>(c->scan_tmp, nb, total_dev));
-    GELL_KERNEL(c, "k_tile_scan", k_tile_scan<<<nb, kThreads, 0, c->stream>>>(in, out, n, c->scan_tmp));
+    GELL_KERNEL(c, "k_tile_scan", k_tile_scan<<<nb, kSortThreads, 0, c->stream>>>(in, out, n, c->scan_tmp));
     return GELL_OK;
 }
 
