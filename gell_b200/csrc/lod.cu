@@ -1072,8 +1072,12 @@ __global__ void k_source_lines_batch(const SrcItem* items, int nitems) {
             float* pl = it.p + (long long)line * it.P;
             const float* rl = it.rate + (long long)line * it.P;
             for (int j = lane; j < N; j += 32) {
-                const float v = (bl || j < 2 || j > N - 3) ? it.b : pl[j];
-                pl[j] = __fdiv_rn(v, __fmaf_rn(-rl[j], it.dt, 1.f));
+                // as k_source_lines: a zero rate divides by exactly 1, so interior elements
+                // without uptake are left as they are
+                const bool edge = bl || j < 2 || j > N - 3;
+                const float r = rl[j], pv = pl[j];
+                if (!edge && r == 0.f) continue;
+                pl[j] = __fdiv_rn(edge ? it.b : pv, __fmaf_rn(-r, it.dt, 1.f));
             }
         }
     }
@@ -1138,11 +1142,14 @@ __global__ void k_source_lines(SrcArgs a) {
                     pv[k] = j < N ? pl[j] : 0.f;
                     rv[k] = j < N ? rl[j] : 0.f;
                 }
+                // where the rate is 0 the divisor is exactly 1 and an interior element keeps its
+                // value: only boundary elements and elements with uptake are divided and written
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
                     const int j = j0 + 32 * k + lane;
-                    if (j < N) {
-                        const float v = (bl || j < 2 || j > N - 3) ? a.b[s] : pv[k];
+                    const bool edge = bl || j < 2 || j > N - 3;
+                    if (j < N && (edge || rv[k] != 0.f)) {
+                        const float v = edge ? a.b[s] : pv[k];
                         pl[j] = __fdiv_rn(v, __fmaf_rn(-rv[k], a.dt, 1.f));
                     }
                 }
