@@ -121,3 +121,47 @@ def test_batched_lod_matches_members_stepped_alone():
     np.testing.assert_array_equal(alone[2].field(1).view(np.uint32), together[2].field(1).view(np.uint32))
     for m in alone + together:
         m.close()
+
+
+def test_batched_steps_with_empty_and_substrate_free_members():
+    """Batched steps (every member's mechanics and LOD as one launch per kernel) when a member holds
+    no cells (its uptake map is still cleared) and another has no substrate (no uptake map, no LOD):
+    each member gives what it gives stepped alone, across birth and death."""
+    def make():
+        ms = [member(0, 40, 2000), member(1, 48, 3000), member(2, 56, 4000)]
+        empty = gb.Simulation(voxel_num=44, voxel_length=10.0, max_cell_num=65536, rng_mode=gb.GELL_RNG_PHILOX,
+                              seed=77)
+        empty.add_substrate(gb.oxygen())
+        empty.set_field(0, random_field(44, seed=78))
+        bare = gb.Simulation(voxel_num=36, voxel_length=10.0, max_cell_num=65536, rng_mode=gb.GELL_RNG_PHILOX,
+                             seed=79)
+        bare.import_cells(gb.seed_ki67_states(ball_cells(36, 10.0, 1500, seed=80, radius_frac=0.3, outside=0), 81))
+        return ms + [empty, bare]
+
+    alone, together = make(), make()
+    with gb.Ensemble(together) as ens:
+        ens.configure(branches=2, sweep_warps=0)
+        ens.set_batched(True)
+        for a in alone:
+            for _ in range(4):
+                a.mechanics_step(3)
+        ens.run_mechanics(4, 3)
+        for a, b in zip(alone, together):
+            a.CellBirth_kernel()
+            b.CellBirth_kernel()
+        for a in alone:
+            for _ in range(3):
+                a.mechanics_step(3)
+        ens.run_mechanics(3, 3)
+        for a, b in zip(alone, together):
+            a.CellDeath_kernel()
+            b.CellDeath_kernel()
+        ens.sync()
+    for i, (a, b) in enumerate(zip(alone, together)):
+        assert a.count() == b.count(), i
+        np.testing.assert_array_equal(raw(a.export_cells()), raw(b.export_cells()))
+        if i < 4:
+            np.testing.assert_array_equal(a.field(0).view(np.uint32), b.field(0).view(np.uint32))
+    assert together[3].count() == 0
+    for m in alone + together:
+        m.close()
