@@ -362,11 +362,13 @@ gell_status gell_reference_spheroid(const gell_params* p, int n, float cell_radi
  * and tile widths 0, 2, 1, then the batched LOD, with real steps of the members (2 per trial, plus
  * one first step; the total is returned in *steps_taken) and keeps the fastest.  The members must
  * outlive the ensemble and live on the device that is current when it is created.
- * gell_ensemble_set_batched (0 or 1, default 0): every captured step runs the members' FM_update and
- * PreLOD on the branches, then the LOD substeps of ALL members as one launch per sweep axis (and one
- * for the uptake source) over a device-side list of every member's line tiles; grid edges up to 256.
- * Results are identical either way.  gell_ensemble_get_batched reports the setting (after a tune,
- * whether the tuner chose it).
+ * gell_ensemble_set_batched (0 or 1, default 0): every captured step runs the FM_update and PreLOD
+ * of ALL members as one launch per kernel (keys, each radix-sort pass, gather, force and move,
+ * uptake map; up to 64 members with up to 4 substrates each, larger ensembles run these on the
+ * branches), then their LOD substeps as one launch per sweep axis (and one for the uptake source)
+ * over a device-side list of every member's line tiles; grid edges up to 256.  Results are
+ * identical either way.  gell_ensemble_get_batched reports the setting (after a tune, whether the
+ * tuner chose it).
  */
 typedef struct gell_ensemble gell_ensemble;
 gell_status gell_ensemble_create(gell_ctx* const* members, int count, gell_ensemble** out);
