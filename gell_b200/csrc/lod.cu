@@ -1186,6 +1186,21 @@ int num_sms() {
     return g_num_sms;
 }
 
+// k_source_lines: as many CTAs as are resident at once (one wave), each warp walking its share of
+// the listed lines; a second, partial wave would start its lines only as the first wave's CTAs end
+int g_source_ctas = 0;
+int source_ctas() {
+    if (!g_source_ctas) {
+        int occ = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_source_lines, 256, 0) != cudaSuccess || occ < 1) {
+            cudaGetLastError();
+            occ = 4;
+        }
+        g_source_ctas = num_sms() * occ;
+    }
+    return g_source_ctas;
+}
+
 }  // namespace
 
 gell_status prelod(gell_ctx* c, int sub) {
@@ -1275,7 +1290,7 @@ static gell_status lod_solver_ring(gell_ctx* c, const LodArgs& ax, const LodArgs
     sa.g = c->g;
     sa.dt = c->P.diffusion_dt;
     for (int k = 0; k < substeps; ++k) {
-        GELL_KERNEL(c, "k_source_lines", k_source_lines<<<num_sms() * 8, 256, 0, strm>>>(sa));
+        GELL_KERNEL(c, "k_source_lines", k_source_lines<<<source_ctas(), 256, 0, strm>>>(sa));
         if (hint) {
             GELL_KERNEL(c, "k_sweep_x", k_sweep_ring<0, true><<<gx, W * 32, smem, strm>>>(ax, R, L));
             GELL_KERNEL(c, "k_sweep_y", k_sweep_ring<1, true><<<gy, W * 32, smem, strm>>>(ay, R, L));
@@ -1372,7 +1387,7 @@ static gell_status lod_solver_range(gell_ctx* c, int s0, int s1, int substeps, c
     sa.g = c->g;
     sa.dt = c->P.diffusion_dt;
     for (int k = 0; k < substeps; ++k) {
-        GELL_KERNEL(c, "k_source_lines", k_source_lines<<<num_sms() * 8, 256, 0, strm>>>(sa));
+        GELL_KERNEL(c, "k_source_lines", k_source_lines<<<source_ctas(), 256, 0, strm>>>(sa));
         GELL_KERNEL(c, "k_sweep_x", k_sweep<0><<<gx, w * 64, smem, strm>>>(ax));
         GELL_KERNEL(c, "k_sweep_y", k_sweep<1><<<gy, w * 64, smem, strm>>>(ay));
         GELL_KERNEL(c, "k_sweep_z", k_sweep<2><<<gz, w * 64, smem, strm>>>(az));
