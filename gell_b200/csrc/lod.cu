@@ -1057,29 +1057,57 @@ __global__ void __launch_bounds__(64 * kBatchWarps, 1) k_sweep_batch(const __gri
 
 // Setboundary + meshupdatekernel on the listed uptake lines of every item (k_source_lines over
 // many grids).
+// The listed lines of all items form one sequence (item by item, each item's list in order) that
+// the warps share round-robin: line g of the sequence goes to warp g mod (warps in the grid), so
+// every warp takes about the same number of lines whatever the items' counts.  The counts live on
+// the device (PreLOD builds the lists), so each warp reads them 32 items at a time and scans them;
+// a line's item is the last one whose first index is not after it.  A line (N <= 256 here) is one
+// batch of 8 loads per lane.
 __global__ void k_source_lines_batch(const SrcItem* items, int nitems) {
     const int lane = threadIdx.x & 31;
     const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (int s = 0; s < nitems; ++s) {
-        const SrcItem& it = items[s];
-        const int N = it.N;
-        const int cnt = *it.count;
-        for (long long li = gw; li < cnt; li += nw) {
+    long long base = 0;  // lines of the items before this group of 32
+    for (int i0 = 0; i0 < nitems; i0 += 32) {
+        const int s = i0 + lane;
+        const int cnt = s < nitems ? *items[s].count : 0;
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int excl = incl - cnt;
+        const int gtot = __shfl_sync(FULL, incl, 31);
+        for (long long g = base + ((gw - base) % nw + nw) % nw; g < base + gtot; g += nw) {
+            const int r = (int)(g - base);
+            const unsigned m = __ballot_sync(FULL, s < nitems && excl <= r);
+            const int src = 31 - __clz(m);
+            const int li = r - __shfl_sync(FULL, excl, src);
+            const SrcItem& it = items[i0 + src];
+            const int N = it.N;
             const int line = it.list[li];
             const int y = line % N, z = line / N;
             const bool bl = y < 2 || y >= N - 2 || z < 2 || z >= N - 2;
             float* pl = it.p + (long long)line * it.P;
             const float* rl = it.rate + (long long)line * it.P;
-            for (int j = lane; j < N; j += 32) {
-                // as k_source_lines: a zero rate divides by exactly 1, so interior elements
-                // without uptake are left as they are
+            float pv[8], rv[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int j = 32 * k + lane;
+                pv[k] = j < N ? pl[j] : 0.f;
+                rv[k] = j < N ? rl[j] : 0.f;
+            }
+            // as k_source_lines: a zero rate divides by exactly 1, so interior elements without
+            // uptake are left as they are
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int j = 32 * k + lane;
                 const bool edge = bl || j < 2 || j > N - 3;
-                const float r = rl[j], pv = pl[j];
-                if (!edge && r == 0.f) continue;
-                pl[j] = __fdiv_rn(edge ? it.b : pv, __fmaf_rn(-r, it.dt, 1.f));
+                if (j < N && (edge || rv[k] != 0.f)) pl[j] = __fdiv_rn(edge ? it.b : pv[k], __fmaf_rn(-rv[k], it.dt, 1.f));
             }
         }
+        base += gtot;
     }
 }
 
@@ -1186,20 +1214,23 @@ int num_sms() {
     return g_num_sms;
 }
 
-// k_source_lines: as many CTAs as are resident at once (one wave), each warp walking its share of
-// the listed lines; a second, partial wave would start its lines only as the first wave's CTAs end
-int g_source_ctas = 0;
-int source_ctas() {
-    if (!g_source_ctas) {
+// The uptake-source kernels: as many CTAs of 256 threads as are resident at once (one wave), each
+// warp walking its share of the listed lines; a second, partial wave would start its lines only as
+// the first wave's CTAs end.  `cache` keeps the count per kernel.
+int one_wave_ctas(const void* kern, int* cache) {
+    if (!*cache) {
         int occ = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_source_lines, 256, 0) != cudaSuccess || occ < 1) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 256, 0) != cudaSuccess || occ < 1) {
             cudaGetLastError();
             occ = 4;
         }
-        g_source_ctas = num_sms() * occ;
+        *cache = num_sms() * occ;
     }
-    return g_source_ctas;
+    return *cache;
 }
+int g_source_ctas = 0, g_source_batch_ctas = 0;
+int source_ctas() { return one_wave_ctas((const void*)k_source_lines, &g_source_ctas); }
+int source_batch_ctas() { return one_wave_ctas((const void*)k_source_lines_batch, &g_source_batch_ctas); }
 
 }  // namespace
 
@@ -1494,7 +1525,7 @@ gell_status lod_batch_run(LodBatch* b, cudaStream_t st, int substeps) {
         return (int)(want < num_sms() ? want : num_sms());
     };
     for (int k = 0; k < substeps; ++k) {
-        GELL_KERNEL(c, "k_source_lines", k_source_lines_batch<<<num_sms() * 8, 256, 0, st>>>(b->d_src, b->nitems));
+        GELL_KERNEL(c, "k_source_lines", k_source_lines_batch<<<source_batch_ctas(), 256, 0, st>>>(b->d_src, b->nitems));
         GELL_KERNEL(c, "k_sweep_x", k_sweep_batch<0><<<grid(a.total[0]), W * 64, smem, st>>>(a, b->Bmax));
         GELL_KERNEL(c, "k_sweep_y", k_sweep_batch<1><<<grid(a.total[1]), W * 64, smem, st>>>(a, b->Bmax));
         GELL_KERNEL(c, "k_sweep_z", k_sweep_batch<2><<<grid(a.total[2]), W * 64, smem, st>>>(a, b->Bmax));
